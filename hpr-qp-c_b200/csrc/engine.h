@@ -1,0 +1,52 @@
+// Internal interface between the host outer loop (solver.cpp) and the CUDA
+// engine (engine.cu).  Not installed; no CUDA types cross this header.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "shared/types.h"
+
+namespace hpr {
+
+struct Engine;  // device-resident problem + iterate state (engine.cu)
+
+struct SetupInfo {
+    double sigma;
+    double lambda_max_A;
+    double lambda_max_Q;
+    int Q_is_diag;
+    int noC;
+    size_t n, m;
+    HPRQPScaling scaling_scalars;  // only the scalar fields are filled
+};
+
+// Upload, scale (Ruiz x10 + Pock-Chambolle), power iteration, sigma0.
+// Mirrors solve_gpu's setup sequence (reference src/gpu/solver.cu:167-210).
+HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, Engine **out,
+                          SetupInfo *info);
+void engine_destroy(Engine *e);
+
+// Backend operations with the semantics of the reference's
+// HPRQPSolverBackendOps (src/shared/solver_backend.h:18-36).
+HPRQPStatus engine_residuals(Engine *e, HPRQPResiduals *res, size_t iter);
+HPRQPStatus engine_iteration_step(Engine *e, size_t inner, int to_check);
+HPRQPStatus engine_m_norm(Engine *e, double *out);
+HPRQPStatus engine_update_sigma(Engine *e, const HPRQPRestart *rst, const HPRQPResiduals *res,
+                                double *sigma_out);
+HPRQPStatus engine_restart_apply(Engine *e);
+HPRQPStatus engine_copy_output(Engine *e, double *x, double *w, double *z, double *y);
+double engine_sigma(const Engine *e);
+
+// Diagnostics used by tests and the benchmark.
+struct ScaleDump {
+    double *row_norm, *col_norm, *q_val, *a_val, *at_val, *c, *l, *u, *AL, *AU;
+    double norm_b_org, norm_c_org, norm_b, norm_c;
+};
+HPRQPStatus engine_dump_scaling(Engine *e, ScaleDump *d);
+
+// Kernel launch counter (process-wide, all engine kernels).
+uint64_t launch_count();
+void count_launch(uint64_t k = 1);
+
+}  // namespace hpr

@@ -1,0 +1,316 @@
+"""ctypes access to the CPU checkers (test infrastructure only).
+
+* ``liboracle.so``: this project's serial C restatement of the reference
+  algorithm (oracle/hprqp_oracle.c), built by ``make -C oracle``.
+* ``_ref/libhprqp_ref_cpu.so``: the reference's own CPU backend compiled from
+  its sources by ``make -C oracle ref`` (only possible where the reference
+  sources exist; the built library travels with the repository snapshot).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline legs use
+this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "lib" / "liboracle.so"
+REF_CPU_LIB = HERE / "_ref" / "libhprqp_ref_cpu.so"
+
+MODE_GPU_REF = 0
+MODE_CPU_REF = 1
+
+c_size_p = ctypes.POINTER(ctypes.c_size_t)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+
+
+class _OracleResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("iter", ctypes.c_size_t),
+        ("iter_4", ctypes.c_size_t),
+        ("iter_6", ctypes.c_size_t),
+        ("primal_obj", ctypes.c_double),
+        ("residuals", ctypes.c_double),
+        ("gap", ctypes.c_double),
+        ("err_rp", ctypes.c_double),
+        ("err_rd", ctypes.c_double),
+        ("dual_obj", ctypes.c_double),
+        ("sigma", ctypes.c_double),
+        ("lambda_max_A", ctypes.c_double),
+        ("lambda_max_Q", ctypes.c_double),
+        ("Q_is_diag", ctypes.c_int),
+        ("noC", ctypes.c_int),
+        ("restarts", ctypes.c_size_t),
+        ("time", ctypes.c_double),
+    ]
+
+
+class _OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("stoptol", ctypes.c_double),
+        ("max_iter", ctypes.c_size_t),
+        ("time_limit", ctypes.c_double),
+        ("check_iter", ctypes.c_size_t),
+        ("print_frequency", ctypes.c_int),
+        ("use_scaling", ctypes.c_int),
+        ("mode", ctypes.c_int),
+    ]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def build_oracle() -> None:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not ORACLE_LIB.exists():
+            build_oracle()
+        _lib = ctypes.CDLL(str(ORACLE_LIB))
+        _lib.oracle_build.restype = ctypes.c_int
+        _lib.oracle_solve.restype = ctypes.c_int
+        _lib.oracle_model_n.restype = ctypes.c_size_t
+        _lib.oracle_model_m.restype = ctypes.c_size_t
+        _lib.oracle_model_q_nnz.restype = ctypes.c_size_t
+        _lib.oracle_model_a_nnz.restype = ctypes.c_size_t
+        for name in ("oracle_model_n", "oracle_model_m", "oracle_model_q_nnz", "oracle_model_a_nnz",
+                     "oracle_model_free"):
+            getattr(_lib, name).argtypes = [ctypes.c_void_p]
+    return _lib
+
+
+def _sz(a: np.ndarray):
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return a, a.ctypes.data_as(c_size_p)
+
+
+def _db(a: Optional[np.ndarray]):
+    if a is None:
+        return None, None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(c_double_p)
+
+
+class OracleModel:
+    """A preprocessed model inside the C oracle."""
+
+    def __init__(self, inst):
+        L = lib()
+        keep = []
+
+        def sz(a):
+            arr, p = _sz(a)
+            keep.append(arr)
+            return p
+
+        def db(a):
+            arr, p = _db(a)
+            keep.append(arr)
+            return p
+
+        handle = ctypes.c_void_p()
+        st = L.oracle_build(
+            ctypes.c_size_t(inst.n), ctypes.c_size_t(inst.Q.nnz), sz(inst.Q.indptr), sz(inst.Q.indices),
+            db(inst.Q.data), ctypes.c_size_t(inst.m), ctypes.c_size_t(inst.A.nnz), sz(inst.A.indptr),
+            sz(inst.A.indices), db(inst.A.data), db(inst.c), db(inst.AL if inst.m else np.zeros(1)),
+            db(inst.AU if inst.m else np.zeros(1)), db(inst.l), db(inst.u),
+            ctypes.c_double(inst.obj_constant), ctypes.byref(handle))
+        if st != 0:
+            raise ValueError(f"oracle_build failed with status {st}")
+        self.handle = handle
+        self.n = int(L.oracle_model_n(handle))
+        self.m = int(L.oracle_model_m(handle))
+
+    def __del__(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            lib().oracle_model_free(self.handle)
+            self.handle = None
+
+    def export(self):
+        L = lib()
+        qn = int(L.oracle_model_q_nnz(self.handle))
+        an = int(L.oracle_model_a_nnz(self.handle))
+        q_rp = np.zeros(self.n + 1, np.uint64)
+        q_ci = np.zeros(max(qn, 1), np.uint64)
+        q_v = np.zeros(max(qn, 1))
+        a_rp = np.zeros(self.m + 1, np.uint64)
+        a_ci = np.zeros(max(an, 1), np.uint64)
+        a_v = np.zeros(max(an, 1))
+        c = np.zeros(self.n)
+        l = np.zeros(self.n)
+        u = np.zeros(self.n)
+        AL = np.zeros(max(self.m, 1))
+        AU = np.zeros(max(self.m, 1))
+        L.oracle_model_export(self.handle, *[a.ctypes.data_as(c_size_p if a.dtype == np.uint64 else c_double_p)
+                                             for a in (q_rp, q_ci, q_v, a_rp, a_ci, a_v, c, AL, AU, l, u)])
+        return dict(q_indptr=q_rp.astype(np.int64), q_indices=q_ci[:qn].astype(np.int64), q_data=q_v[:qn],
+                    a_indptr=a_rp.astype(np.int64), a_indices=a_ci[:an].astype(np.int64), a_data=a_v[:an],
+                    c=c, l=l, u=u, AL=AL[:self.m], AU=AU[:self.m])
+
+    def solve(self, stoptol=1e-8, max_iter=2147483647, time_limit=3600.0, check_iter=100,
+              print_frequency=-1, use_scaling=True, mode=MODE_GPU_REF):
+        p = _OracleParams(stoptol, max_iter, time_limit, check_iter, print_frequency, int(use_scaling), mode)
+        r = _OracleResult()
+        x = np.zeros(max(self.n, 1))
+        w = np.zeros(max(self.n, 1))
+        z = np.zeros(max(self.n, 1))
+        y = np.zeros(max(self.m, 1))
+        lib().oracle_solve(self.handle, ctypes.byref(p), ctypes.byref(r), x.ctypes.data_as(c_double_p),
+                           y.ctypes.data_as(c_double_p), z.ctypes.data_as(c_double_p), w.ctypes.data_as(c_double_p))
+        out = {name: getattr(r, name) for name, _ in _OracleResult._fields_}
+        out.update(x=x[:self.n], y=y[:self.m], z=z[:self.n], w=w[:self.n])
+        return out
+
+    def setup(self, use_scaling=True, mode=MODE_GPU_REF):
+        out = np.zeros(5)
+        st = lib().oracle_setup(self.handle, int(use_scaling), mode, out.ctypes.data_as(c_double_p))
+        if st != 0:
+            raise ValueError(st)
+        return dict(sigma=out[0], lambda_max_A=out[1], lambda_max_Q=out[2], Q_is_diag=int(out[3]), noC=int(out[4]))
+
+    def scale(self, use_scaling=True, mode=MODE_GPU_REF):
+        L = lib()
+        qn = int(L.oracle_model_q_nnz(self.handle))
+        an = int(L.oracle_model_a_nnz(self.handle))
+        arrs = dict(row_norm=np.zeros(max(self.m, 1)), col_norm=np.zeros(max(self.n, 1)),
+                    q_data=np.zeros(max(qn, 1)), a_data=np.zeros(max(an, 1)), c=np.zeros(max(self.n, 1)),
+                    l=np.zeros(max(self.n, 1)), u=np.zeros(max(self.n, 1)), AL=np.zeros(max(self.m, 1)),
+                    AU=np.zeros(max(self.m, 1)), scalars=np.zeros(4))
+        st = L.oracle_scale(self.handle, int(use_scaling), mode,
+                            *[arrs[k].ctypes.data_as(c_double_p) for k in
+                              ("row_norm", "col_norm", "q_data", "a_data", "c", "l", "u", "AL", "AU", "scalars")])
+        if st != 0:
+            raise ValueError(st)
+        arrs["row_norm"] = arrs["row_norm"][:self.m]
+        arrs["AL"] = arrs["AL"][:self.m]
+        arrs["AU"] = arrs["AU"][:self.m]
+        arrs["q_data"] = arrs["q_data"][:qn]
+        arrs["a_data"] = arrs["a_data"][:an]
+        return arrs
+
+    def kkt(self, x, y, z):
+        out = np.zeros(6)
+        xa, xp = _db(x)
+        ya, yp = _db(y if self.m else np.zeros(1))
+        za, zp = _db(z)
+        lib().oracle_kkt(self.handle, xp, yp, zp, out.ctypes.data_as(c_double_p))
+        return dict(err_rp=out[0], err_rd=out[1], gap=out[2], primal_obj=out[3], dual_obj=out[4], kkt=out[5])
+
+
+def matvec(indptr, indices, data, x):
+    indptr_a, ip = _sz(indptr)
+    indices_a, ii = _sz(indices if len(indices) else np.zeros(1))
+    data_a, dp = _db(data if len(data) else np.zeros(1))
+    xa, xp = _db(x if len(x) else np.zeros(1))
+    nrow = len(indptr) - 1
+    y = np.zeros(max(nrow, 1))
+    lib().oracle_csr_matvec(ctypes.c_size_t(nrow), ip, ii, dp, xp, y.ctypes.data_as(c_double_p))
+    return y[:nrow]
+
+
+# --------------------------------------------------------------------------
+# the reference's own CPU library (oracle/_ref), through its hprqp_* ABI
+# --------------------------------------------------------------------------
+
+_ref: Optional[ctypes.CDLL] = None
+
+
+def ref_available() -> bool:
+    return REF_CPU_LIB.exists()
+
+
+def ref_lib() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(str(REF_CPU_LIB))
+        _ref.hprqp_status_name.restype = ctypes.c_char_p
+        for name in ("hprqp_results_x_data", "hprqp_results_y_data", "hprqp_results_z_data",
+                     "hprqp_results_w_data"):
+            getattr(_ref, name).restype = c_double_p
+            getattr(_ref, name).argtypes = [ctypes.c_void_p]
+        for name in ("hprqp_results_iter", "hprqp_results_iter_4", "hprqp_results_iter_6",
+                     "hprqp_results_num_variables", "hprqp_results_num_constraints"):
+            getattr(_ref, name).restype = ctypes.c_size_t
+            getattr(_ref, name).argtypes = [ctypes.c_void_p]
+        for name in ("hprqp_results_time", "hprqp_results_objective", "hprqp_results_residual",
+                     "hprqp_results_gap"):
+            getattr(_ref, name).restype = ctypes.c_double
+            getattr(_ref, name).argtypes = [ctypes.c_void_p]
+        _ref.hprqp_params_set_stoptol.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        _ref.hprqp_params_set_time_limit.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        for name in ("hprqp_params_set_max_iter", "hprqp_params_set_check_iter"):
+            getattr(_ref, name).argtypes = [ctypes.c_void_p, ctypes.c_size_t]
+        for name in ("hprqp_params_set_use_gpu", "hprqp_params_set_verbose", "hprqp_params_set_use_scaling",
+                     "hprqp_params_set_print_frequency"):
+            getattr(_ref, name).argtypes = [ctypes.c_void_p, ctypes.c_int]
+        _ref.hprqp_optimize.argtypes = [ctypes.c_void_p] * 3
+    return _ref
+
+
+def ref_solve(inst, stoptol=1e-8, max_iter=2147483647, use_scaling=True, check_iter=100,
+              print_frequency=-1, time_limit=3600.0):
+    """Solve with the reference CPU library (use_gpu=0, polishing off)."""
+    L = ref_lib()
+    keep = []
+
+    def sz(a):
+        arr, p = _sz(a if len(a) else np.zeros(1))
+        keep.append(arr)
+        return p
+
+    def db(a):
+        arr, p = _db(a if len(a) else np.zeros(1))
+        keep.append(arr)
+        return p
+
+    model = ctypes.c_void_p()
+    params = ctypes.c_void_p()
+    res = ctypes.c_void_p()
+    L.hprqp_model_create(ctypes.byref(model))
+    st = L.hprqp_model_build_from_qabc_csr(
+        model, ctypes.c_size_t(inst.n), ctypes.c_size_t(inst.n), ctypes.c_size_t(inst.Q.nnz), sz(inst.Q.indptr),
+        sz(inst.Q.indices), db(inst.Q.data), ctypes.c_size_t(inst.m), ctypes.c_size_t(inst.n),
+        ctypes.c_size_t(inst.A.nnz), sz(inst.A.indptr), sz(inst.A.indices), db(inst.A.data), db(inst.c),
+        db(inst.AL) if inst.m else None, db(inst.AU) if inst.m else None, db(inst.l), db(inst.u),
+        ctypes.c_double(inst.obj_constant))
+    if st != 0:
+        L.hprqp_model_destroy(model)
+        raise ValueError(f"reference build failed: {st}")
+    L.hprqp_params_create(ctypes.byref(params))
+    L.hprqp_params_set_use_gpu(params, 0)
+    L.hprqp_params_set_verbose(params, 0)
+    L.hprqp_params_set_stoptol(params, stoptol)
+    L.hprqp_params_set_max_iter(params, max_iter)
+    L.hprqp_params_set_use_scaling(params, int(use_scaling))
+    L.hprqp_params_set_check_iter(params, check_iter)
+    L.hprqp_params_set_print_frequency(params, print_frequency)
+    L.hprqp_params_set_time_limit(params, time_limit)
+    L.hprqp_results_create(ctypes.byref(res))
+    status = L.hprqp_optimize(model, params, res)
+    n = int(L.hprqp_results_num_variables(res))
+    m = int(L.hprqp_results_num_constraints(res))
+
+    def vec(fn, k):
+        p = fn(res)
+        return np.array([p[i] for i in range(k)]) if (p and k) else np.zeros(0)
+
+    out = dict(status=status, iter=int(L.hprqp_results_iter(res)), iter_4=int(L.hprqp_results_iter_4(res)),
+               iter_6=int(L.hprqp_results_iter_6(res)), primal_obj=L.hprqp_results_objective(res),
+               residuals=L.hprqp_results_residual(res), gap=L.hprqp_results_gap(res),
+               time=L.hprqp_results_time(res),
+               x=vec(L.hprqp_results_x_data, n), y=vec(L.hprqp_results_y_data, m),
+               z=vec(L.hprqp_results_z_data, n), w=vec(L.hprqp_results_w_data, n))
+    L.hprqp_results_destroy(res)
+    L.hprqp_params_destroy(params)
+    L.hprqp_model_destroy(model)
+    return out
