@@ -31,6 +31,24 @@ static std::atomic<uint64_t> g_launches{0};
 uint64_t launch_count() { return g_launches.load(); }
 void count_launch(uint64_t k) { g_launches.fetch_add(k); }
 
+static bool trace_on()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *v = getenv("HPRQP_B200_TRACE");
+        on = (v && v[0] == '1') ? 1 : 0;
+    }
+    return on == 1;
+}
+#define HPR_TRACE(...)                                  \
+    do {                                                \
+        if (trace_on()) {                               \
+            fprintf(stderr, "[hprqp-b200] " __VA_ARGS__); \
+            fputc('\n', stderr);                       \
+            fflush(stderr);                             \
+        }                                               \
+    } while (0)
+
 #define HPR_CK(call)                                                                         \
     do {                                                                                     \
         cudaError_t err__ = (call);                                                          \
@@ -95,7 +113,7 @@ struct EpiBase {
 #pragma unroll
         for (int k = 0; k < (N > 0 ? N : 1); ++k) a.v[k] = 0.0;
     }
-    __device__ void ops(int *o) const
+    __host__ __device__ void ops(int *o) const
     {
         for (int k = 0; k < N; ++k) o[k] = kSum;
     }
@@ -280,7 +298,7 @@ struct EpiStore : EpiBase<0> {
 // A x_bar: Ax, s = proj(Ax), Rp; slots: max|Rp|, max|Ax*rs|, sum ybar*s
 struct EpiResA : EpiBase<3> {
     DState S;
-    __device__ void ops(int *o) const
+    __host__ __device__ void ops(int *o) const
     {
         o[0] = kMax;
         o[1] = kMax;
@@ -303,7 +321,7 @@ struct EpiResA : EpiBase<3> {
 struct EpiResQ : EpiBase<7> {
     DState S;
     int iter0 = 0;
-    __device__ void ops(int *o) const
+    __host__ __device__ void ops(int *o) const
     {
         o[0] = kMax;
         o[1] = kMax;
@@ -510,7 +528,7 @@ struct EpiPowResid : EpiBase<1> {
 // bound measures before/after scaling: slots max bm, sum bm^2, max|c|, sum c^2
 struct EpiNorms : EpiBase<4> {
     DState S;
-    __device__ void ops(int *o) const
+    __host__ __device__ void ops(int *o) const
     {
         o[0] = kMax;
         o[1] = kSum;
@@ -1081,6 +1099,7 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
             return st;             \
         }                          \
     } while (0)
+    HPR_TRACE("create: set device");
     E_CK(cudaSetDevice(e->device));
     E_CK(cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, e->device));
     E_CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
@@ -1088,6 +1107,7 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
     E_CK(cudaHostGetDevicePointer((void **)&e->dout, e->hout, 0));
     memset(e->hout, 0, sizeof(HostOut));
 
+    HPR_TRACE("create: host alloc ok");
     DState &S = e->S;
     const int n = (int)model->Q.ncol, m = (int)model->A.nrow;
     if (model->Q.ncol > (size_t)INT32_MAX / 2 || model->A.nrow > (size_t)INT32_MAX / 2) {
@@ -1099,6 +1119,7 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
     E_ST(upload_csr(e, model->Q, S.Q));
     E_ST(upload_csr(e, model->A, S.A));
     E_ST(upload_csr(e, model->AT, S.AT));
+    HPR_TRACE("create: csr uploaded");
     // vectors
     double **nvecs[] = {&S.c, &S.l, &S.u, &S.col_norm, &S.x, &S.x_bar, &S.x_hat, &S.w, &S.w_bar, &S.ATy,
                         &S.ATy_bar, &S.ATdy, &S.Qw, &S.Qw_bar, &S.Qx, &S.dQw, &S.QATdy, &S.dx, &S.dw,
@@ -1121,6 +1142,7 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
     int max_blocks = std::max({S.Q.nblocks, S.A.nblocks, S.AT.nblocks, e->num_sms * 4, 1});
     e->partials_len = (size_t)max_blocks * 8 * 2;
     E_ST(dalloc(e, &e->partials, e->partials_len));
+    HPR_TRACE("create: buffers allocated");
     // problem vectors
     E_CK(cudaMemcpyAsync(S.c, model->c, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
     E_CK(cudaMemcpyAsync(S.l, model->l, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
@@ -1137,6 +1159,7 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
         E_CK(cudaStreamSynchronize(e->stream));
     }
 
+    HPR_TRACE("create: vectors uploaded");
     // ---- scaling: reference src/gpu/scale.cu:332-560 --------------------
     EpiNorms en;
     en.S = S;
@@ -1174,6 +1197,7 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
         FinSpec f = spec_of<EpiNorms>(g, 0);
         E_ST(finalize(e, &f, 1, true));
     }
+    HPR_TRACE("create: scaled");
     const double norm_b = m > 0 ? sqrt(e->hout->v[1]) : 0.0;
     const double norm_c = sqrt(e->hout->v[3]);
     info->scaling_scalars.norm_b = norm_b;
@@ -1194,6 +1218,7 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
             S.noC = 5.0 * e->hout->v[0] > 4.0 * (double)n;
         }
     }
+    HPR_TRACE("create: noC done");
     double lambda_Q = 0.0, lambda_A = 0.0;
     {
         const int wgrid = std::max(1, std::min((int)((nn * 32 + kThreads - 1) / kThreads), e->num_sms * 8));
@@ -1204,10 +1229,12 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
         S.q_is_diag = e->hout->v[0] <= 1e-15;
         if (S.q_is_diag) lambda_Q = e->hout->v[1];
     }
+    HPR_TRACE("create: diag done");
     if (!S.q_is_diag) {
         E_ST(power_iteration(e, false, &lambda_Q));
         lambda_Q *= 1.05;
     }
+    HPR_TRACE("create: lambda_Q done");
     E_ST(power_iteration(e, true, &lambda_A));
     lambda_A *= 1.05;
     // the power iteration used pz/pq/ptmp only; iterate vectors are still zero

@@ -1,0 +1,35 @@
+"""Shared test setup: import paths, the `gpu` marker, fixtures."""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT / "oracle"))
+sys.path.insert(0, str(ROOT / "hpr-qp-c_b200" / "python"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def golden():
+    import json
+
+    return json.loads((ROOT / "tests" / "golden" / "reference_cpu.json").read_text())["records"]
+
+
+@pytest.fixture(scope="session")
+def engine_lib():
+    """Builds the engine library if needed and returns the hprqp module."""
+    lib = ROOT / "hpr-qp-c_b200" / "lib" / "libhprqp.so"
+    if not lib.exists():
+        import subprocess
+
+        subprocess.run([sys.executable, str(ROOT / "hpr-qp-c_b200" / "build.py")], check=True)
+    import hprqp
+
+    return hprqp
