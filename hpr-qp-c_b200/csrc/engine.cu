@@ -837,6 +837,7 @@ struct Engine {
     double obj_constant = 0.0, norm_b_org = 0.0, norm_c_org = 0.0;
     // graphs of one step, partial / full
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+    uint64_t step_launches[2] = {0, 0};
     bool use_graphs = true;
 };
 
@@ -857,50 +858,42 @@ static HPRQPStatus dalloc(Engine *e, T **p, size_t count)
     return HPRQP_STATUS_OK;
 }
 
-// Greedy row-block partition (host): maximal runs of rows whose nnz fit in
-// kCap products and kMaxRows rows; longer rows stand alone.
-static void build_row_blocks(const std::vector<int> &rp, std::vector<int2> &blocks)
-{
-    blocks.clear();
-    const int nrow = (int)rp.size() - 1;
-    int r = 0;
-    while (r < nrow) {
-        int r1 = r + 1;
-        long long acc = rp[r + 1] - rp[r];
-        if (acc <= kCap) {
-            while (r1 < nrow && r1 - r < kMaxRows && acc + (rp[r1 + 1] - rp[r1]) <= kCap) {
-                acc += rp[r1 + 1] - rp[r1];
-                ++r1;
-            }
-        }
-        blocks.push_back(make_int2(r, r1));
-        r = r1;
-    }
-}
-
 static HPRQPStatus upload_csr(Engine *e, const HPRQPMatrixCSR &h, DCsr &d)
 {
-    if (h.nnz > (size_t)INT32_MAX || h.nrow > (size_t)INT32_MAX - 1 || h.ncol > (size_t)INT32_MAX)
+    if (h.nnz > (size_t)INT32_MAX - 64 || h.nrow > (size_t)INT32_MAX - 64 || h.ncol > (size_t)INT32_MAX)
         return HPRQP_STATUS_NOT_IMPLEMENTED;  // int32 device indices (reference cuda_common.h:29-50)
     d.nrow = (int)h.nrow;
     d.ncol = (int)h.ncol;
     d.nnz = (int)h.nnz;
-    std::vector<int> rp(h.nrow + 1), ci(h.nnz ? h.nnz : 1);
+    std::vector<int> rp(h.nrow + 1), ci(h.nnz ? h.nnz : 1, 0);
     for (size_t r = 0; r <= h.nrow; ++r) rp[r] = (int)h.row_ptr[r];
     for (size_t k = 0; k < h.nnz; ++k) ci[k] = (int)h.col_ind[k];
-    std::vector<int2> blocks;
-    build_row_blocks(rp, blocks);
+    TilePlan plan;
+    build_tile_plan(rp, plan);
     HPRQPStatus st;
+    const size_t nt = plan.tiles.size(), nc = plan.chunks.size(), nl = plan.long_rows.size();
     if ((st = dalloc(e, &d.rp, rp.size())) || (st = dalloc(e, &d.ci, ci.size())) ||
-        (st = dalloc(e, &d.v, h.nnz ? h.nnz : 1)) || (st = dalloc(e, &d.blocks, blocks.size() ? blocks.size() : 1)))
+        (st = dalloc(e, &d.v, h.nnz ? h.nnz : 1)) || (st = dalloc(e, &d.tiles, nt ? nt : 1)) ||
+        (st = dalloc(e, &d.chunks, nc ? nc : 1)) || (st = dalloc(e, &d.long_rows, nl ? nl : 1)) ||
+        (st = dalloc(e, &d.chunk_partial, nc ? nc : 1)) || (st = dalloc(e, &d.err, 1)))
         return st;
-    d.nblocks = (int)blocks.size();
+    d.ntiles = (int)nt;
+    d.nchunks = (int)nc;
+    d.nlong = (int)nl;
+    d.grid_main = std::max(1, (d.ntiles + kWarps - 1) / kWarps);
+    d.grid_chunk = (d.nchunks + kWarps - 1) / kWarps;
+    d.grid_long = d.nlong ? (d.nlong + kThreads - 1) / kThreads : 0;
+    HPR_CK(cudaMemsetAsync(d.err, 0, sizeof(int), e->stream));
     HPR_CK(cudaMemcpyAsync(d.rp, rp.data(), rp.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
     HPR_CK(cudaMemcpyAsync(d.ci, ci.data(), ci.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
     if (h.nnz)
         HPR_CK(cudaMemcpyAsync(d.v, h.values, h.nnz * sizeof(double), cudaMemcpyHostToDevice, e->stream));
-    if (!blocks.empty())
-        HPR_CK(cudaMemcpyAsync(d.blocks, blocks.data(), blocks.size() * sizeof(int2), cudaMemcpyHostToDevice,
+    if (nt)
+        HPR_CK(cudaMemcpyAsync(d.tiles, plan.tiles.data(), nt * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
+    if (nc)
+        HPR_CK(cudaMemcpyAsync(d.chunks, plan.chunks.data(), nc * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
+    if (nl)
+        HPR_CK(cudaMemcpyAsync(d.long_rows, plan.long_rows.data(), nl * sizeof(int2), cudaMemcpyHostToDevice,
                                e->stream));
     // the host vectors die at return: make the copies complete first
     HPR_CK(cudaStreamSynchronize(e->stream));
@@ -914,12 +907,26 @@ static int ew_grid(const Engine *e, int len)
 }
 
 template <class Epi>
-static void launch_rb(Engine *e, const DCsr &M, const double *x, Epi epi)
+static void launch_rb_at(Engine *e, const DCsr &M, const double *x, Epi epi, size_t poff)
 {
     if (M.nrow == 0) return;
-    if (Epi::NRED > 0) epi.partials = e->partials;
-    k_rowblock<Epi><<<M.nblocks, kThreads, 0, e->stream>>>(M, x, epi);
+    epi.partials = e->partials + poff;
+    if (M.nchunks) {
+        k_chunks<<<M.grid_chunk, kThreads, 0, e->stream>>>(M, x);
+        count_launch();
+    }
+    k_spmv<Epi><<<M.grid_main, kThreads, 0, e->stream>>>(M, x, epi);
     count_launch();
+    if (M.nlong) {
+        k_long_epi<Epi><<<M.grid_long, kThreads, 0, e->stream>>>(M, epi);
+        count_launch();
+    }
+}
+
+template <class Epi>
+static void launch_rb(Engine *e, const DCsr &M, const double *x, Epi epi)
+{
+    launch_rb_at(e, M, x, epi, 0);
 }
 
 template <class Epi>
@@ -972,15 +979,6 @@ static FinSpec spec_of(int nblocks, int out_off, size_t poff = 0)
     return FinSpec{poff, nblocks, Epi::NRED, opsmask_of(ops, Epi::NRED), out_off};
 }
 
-// rowblock launch writing partials at an offset
-template <class Epi>
-static void launch_rb_at(Engine *e, const DCsr &M, const double *x, Epi epi, size_t poff)
-{
-    if (M.nrow == 0) return;
-    epi.partials = e->partials + poff;
-    k_rowblock<Epi><<<M.nblocks, kThreads, 0, e->stream>>>(M, x, epi);
-    count_launch();
-}
 
 // ---- power iteration (reference src/gpu/eigs.cu:185-383) -------------------
 static HPRQPStatus power_iteration(Engine *e, bool is_a, double *lambda_out)
@@ -1024,10 +1022,10 @@ static HPRQPStatus power_iteration(Engine *e, bool is_a, double *lambda_out)
             st.out = S.ptmp;
             launch_rb(e, S.AT, q, st);
             launch_rb(e, S.A, S.ptmp, pp);
-            nb = S.A.nblocks;
+            nb = S.A.npart();
         } else {
             launch_rb(e, S.Q, q, pp);
-            nb = S.Q.nblocks;
+            nb = S.Q.npart();
         }
         FinSpec f = spec_of<EpiPowProd>(nb, 0);
         HPRQPStatus st = finalize(e, &f, 1, true);
@@ -1139,7 +1137,7 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
     S.pq = S.pz + x_al;
     E_ST(dalloc(e, &S.ctl, 1));
     E_CK(cudaMemsetAsync(S.ctl, 0, sizeof(Ctl), e->stream));
-    int max_blocks = std::max({S.Q.nblocks, S.A.nblocks, S.AT.nblocks, e->num_sms * 4, 1});
+    int max_blocks = std::max({S.Q.npart(), S.A.npart(), S.AT.npart(), e->num_sms * 4, 1});
     e->partials_len = (size_t)max_blocks * 8 * 2;
     E_ST(dalloc(e, &e->partials, e->partials_len));
     HPR_TRACE("create: buffers allocated");
@@ -1336,11 +1334,6 @@ static void enqueue_step(Engine *e, int to_check)
     }
 }
 
-static int kernels_per_step(const DState &S)
-{
-    if (S.noC) return 2 + (S.m > 0 ? 1 : 0);
-    return 2 + (S.m > 0 ? 2 : 0);
-}
 
 static HPRQPStatus launch_step(Engine *e, int to_check)
 {
@@ -1355,12 +1348,13 @@ static HPRQPStatus launch_step(Engine *e, int to_check)
         HPR_CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
         enqueue_step(e, to_check);
         HPR_CK(cudaStreamEndCapture(e->stream, &g));
+        e->step_launches[to_check] = launch_count() - before;
         g_launches.store(before);  // captured launches are counted at replay
         HPR_CK(cudaGraphInstantiate(&e->step_graph[to_check], g, 0));
         cudaGraphDestroy(g);
     }
     HPR_CK(cudaGraphLaunch(e->step_graph[to_check], e->stream));
-    count_launch(kernels_per_step(e->S));
+    count_launch(e->step_launches[to_check]);
     return HPRQP_STATUS_OK;
 }
 
@@ -1375,7 +1369,7 @@ HPRQPStatus engine_residuals(Engine *e, HPRQPResiduals *res, size_t iter)
 {
     DState &S = e->S;
     memset(res, 0, sizeof(*res));
-    const size_t off_a = 0, off_q = (size_t)std::max(S.A.nblocks, 1) * 3;
+    const size_t off_a = 0, off_q = (size_t)std::max(S.A.npart(), 1) * 3;
     int nspec = 0;
     FinSpec specs[2];
     if (S.m > 0) {
@@ -1385,7 +1379,7 @@ HPRQPStatus engine_residuals(Engine *e, HPRQPResiduals *res, size_t iter)
         EpiResA ra;
         ra.S = S;
         launch_rb_at(e, S.A, S.x_bar, ra, off_a);
-        specs[nspec++] = spec_of<EpiResA>(S.A.nblocks, 0, off_a);
+        specs[nspec++] = spec_of<EpiResA>(S.A.npart(), 0, off_a);
     } else {
         HPR_CK(cudaMemsetAsync(S.ATdy, 0, (size_t)S.n * sizeof(double), e->stream));
     }
@@ -1393,7 +1387,7 @@ HPRQPStatus engine_residuals(Engine *e, HPRQPResiduals *res, size_t iter)
     rq.S = S;
     rq.iter0 = iter == 0;
     launch_rb_at(e, S.Q, S.x_bar, rq, off_q);
-    specs[nspec++] = spec_of<EpiResQ>(S.Q.nblocks, 8, off_q);
+    specs[nspec++] = spec_of<EpiResQ>(S.Q.npart(), 8, off_q);
     HPRQPStatus st = finalize(e, specs, nspec, true);
     if (st) return st;
     const double *v = e->hout->v;
@@ -1422,22 +1416,22 @@ HPRQPStatus engine_residuals(Engine *e, HPRQPResiduals *res, size_t iter)
 HPRQPStatus engine_m_norm(Engine *e, double *out)
 {
     DState &S = e->S;
-    const size_t o1 = 0, o2 = (size_t)S.Q.nblocks * 4, o3 = o2 + (size_t)std::max(S.AT.nblocks, 1) * 2;
+    const size_t o1 = 0, o2 = (size_t)S.Q.npart() * 4, o3 = o2 + (size_t)std::max(S.AT.npart(), 1) * 2;
     EpiMQdw a;
     a.S = S;
     launch_rb_at(e, S.Q, S.dw, a, o1);
     FinSpec specs[3];
     int ns = 0;
-    specs[ns++] = spec_of<EpiMQdw>(S.Q.nblocks, 0, o1);
+    specs[ns++] = spec_of<EpiMQdw>(S.Q.npart(), 0, o1);
     if (S.m > 0) {
         EpiMATdy b;
         b.S = S;
         launch_rb_at(e, S.AT, S.dy, b, o2);
-        specs[ns++] = spec_of<EpiMATdy>(S.AT.nblocks, 8, o2);
+        specs[ns++] = spec_of<EpiMATdy>(S.AT.npart(), 8, o2);
         EpiMQATdy c;
         c.S = S;
         launch_rb_at(e, S.Q, S.ATdy, c, o3);
-        specs[ns++] = spec_of<EpiMQATdy>(S.Q.nblocks, 16, o3);
+        specs[ns++] = spec_of<EpiMQATdy>(S.Q.npart(), 16, o3);
     }
     HPRQPStatus st = finalize(e, specs, ns, true);
     if (st) return st;
@@ -1506,19 +1500,19 @@ HPRQPStatus engine_update_sigma(Engine *e, const HPRQPRestart *rst, const HPRQPR
     EpiSigDiff d;
     d.S = S;
     const int g = launch_ew(e, std::max(S.n, S.m), d, 0);
-    const size_t o2 = (size_t)g * 2, o3 = o2 + (size_t)S.Q.nblocks * 3;
+    const size_t o2 = (size_t)g * 2, o3 = o2 + (size_t)S.Q.npart() * 3;
     EpiSigQdw q1;
     q1.S = S;
     launch_rb_at(e, S.Q, S.dw, q1, o2);
     FinSpec specs[3];
     int ns = 0;
     specs[ns++] = spec_of<EpiSigDiff>(g, 0, 0);
-    specs[ns++] = spec_of<EpiSigQdw>(S.Q.nblocks, 8, o2);
+    specs[ns++] = spec_of<EpiSigQdw>(S.Q.npart(), 8, o2);
     if (S.m > 0) {
         EpiSigQATdy q2;
         q2.S = S;
         launch_rb_at(e, S.Q, S.ATdy, q2, o3);
-        specs[ns++] = spec_of<EpiSigQATdy>(S.Q.nblocks, 16, o3);
+        specs[ns++] = spec_of<EpiSigQATdy>(S.Q.npart(), 16, o3);
     }
     HPRQPStatus st = finalize(e, specs, ns, true);
     if (st) return st;
@@ -1701,8 +1695,10 @@ static HPRQPStatus spmv_standalone(size_t nrow, size_t ncol, size_t nnz, const s
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
     double total_ms = 0.0;
+    // matrices smaller than 2 x L2 would be timed from L2: evict them first
+    const bool do_flush = nnz * 12 + nrow * 4 < ((size_t)256 << 20);
     for (int r = 0; r < reps; ++r) {
-        cudaMemsetAsync(flush, r & 0xff, flush_bytes, e->stream);
+        if (do_flush) cudaMemsetAsync(flush, r & 0xff, flush_bytes, e->stream);
         cudaEventRecord(ev0, e->stream);
         launch_rb(e, M, dx, ep);
         cudaEventRecord(ev1, e->stream);

@@ -21,8 +21,9 @@ extern "C" {
  * src/gpu/spmv.cu:25-39, 511-659).  Host arrays in, host array out; the
  * kernel is replayed `reps` times (>= 1) and, when ms_per_spmv is non-NULL,
  * the mean device time of one product (CUDA events) is returned there.
- * Timed products are separated by a 256 MiB buffer write so each one reads
- * the matrix from HBM, not L2. */
+ * A matrix whose stream is smaller than 256 MiB is evicted from L2 (a
+ * 256 MiB buffer write) before every timed product, so each product reads it
+ * from HBM; larger matrices do not fit in L2 and are timed back to back. */
 HPRQPStatus hprqp_b200_spmv(size_t nrow, size_t ncol, size_t nnz, const size_t *row_ptr,
                             const size_t *col_ind, const double *values, const double *x, double *y,
                             int reps, double *ms_per_spmv);
