@@ -1,0 +1,1458 @@
+// Batched HPR-QP solver: one persistent kernel solves thousands of
+// independent QPs.
+//
+// Each CTA takes instances from a global work queue (largest first, so the
+// tail of the batch is made of short jobs) and runs the complete method for
+// its instance: Ruiz + Pock-Chambolle scaling, power iterations, HPR steps,
+// residual checks, restarts and the sigma update, with the control logic of
+// the reference's outer loop (src/shared/solver_backend.c:338-569,
+// src/cpu/control.c:231-411) executed by thread 0 on CTA-shared scalars and
+// every vector operation spread over the CTA.  Convergence, restarts and
+// sigma are therefore per instance, and an instance that converges frees
+// its CTA for the next one immediately.
+//
+// Inside a CTA, y = M x runs over 32-row warp tiles whose lane-group width
+// is chosen per tile from the instance's own row lengths (the per-instance
+// SpMV autotuner); every reduction is folded in a fixed order, so each
+// instance's result is independent of which CTA solved it.
+#include "engine.h"
+#include "hprqp_batch.h"
+#include "hprqp.h"
+#include "rowblock.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+namespace hpr {
+
+#ifndef HPR_BATCH_THREADS
+#define HPR_BATCH_THREADS 1024
+#endif
+#ifndef HPR_BATCH_LD
+#define HPR_BATCH_LD __ldg  // instance matrices are re-read every iteration: keep them in L2
+#endif
+#ifndef HPR_BATCH_VEC_SMEM
+#define HPR_BATCH_VEC_SMEM 1
+#endif
+constexpr int kBT = HPR_BATCH_THREADS;  // threads per CTA of the batch kernel
+constexpr int kBW = kBT / 32;
+constexpr int kWin = 256;  // entries per warp window of the flat SpMV (8 per lane)
+constexpr size_t kScratchBytes = (size_t)kBW * kWin * sizeof(double);
+constexpr size_t kSmemLimit = 220 * 1024;  // dynamic shared memory of the batch kernel
+
+struct BInst {
+    long long q_nz, a_nz, at_nz;  // first entry of the instance's matrices
+    int q_rp, a_rp, at_rp;        // first row pointer
+    int var, row;                 // first variable / row in the packed vectors
+    int n, m;
+    double obj_constant;
+};
+
+struct BatchArgs {
+    int K;
+    const BInst *inst;
+    const int *order;
+    int *counter;
+    const int *q_rp, *q_ci, *a_rp, *a_ci, *at_rp, *at_ci;
+    const double *q_v0, *a_v0, *at_v0, *c0, *l0, *u0, *AL0, *AU0;
+    double *q_v, *a_v, *at_v;  // scaled copies
+    double *ws;                // per-CTA workspace
+    size_t ws_stride;
+    int nmax, mmax;
+    int vec_smem;              // 1: the gathered vectors live in shared memory
+    // parameters
+    double stoptol;
+    long long max_iter;
+    double time_limit;
+    int check_iter;
+    int print_frequency;
+    int use_scaling;
+    unsigned long long t_start;  // globaltimer at launch (ns), set by CTA 0
+    // outputs (packed like the inputs)
+    double *x, *y, *z, *w;
+    int *status;
+    long long *iters;
+    double *pobj, *resid, *gap;
+    int *restarts;
+    unsigned long long *phase_clk;  // optional [grid x 8] clock64 totals per phase
+    unsigned char *active_x;  // 1 = variable at a bound (for the adjoint)
+    unsigned char *active_r;  // 1 = row at a bound
+};
+
+// optional per-CTA phase clocks: 0 load+scale, 1 setup norms/diag, 2 power
+// iterations, 3 steps, 4 residuals, 5 m-norm, 6 sigma+restart, 7 total
+#define PHASE_T0() long long _pt0 = clock64()
+#define PHASE_ADD(k)                                                                       \
+    do {                                                                                   \
+        if (B.phase_clk && threadIdx.x == 0)                                               \
+            B.phase_clk[blockIdx.x * 8 + (k)] += (unsigned long long)(clock64() - _pt0);   \
+        _pt0 = clock64();                                                                  \
+    } while (0)
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// local CSR view of one instance's matrix
+struct LCsr {
+    int nrow;
+    const int *rp;
+    const int *ci;
+    const double *v;
+};
+
+__device__ __forceinline__ double clampd(double v, double lo, double hi)
+{
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+// fold per-thread values over the CTA; every thread gets the results
+template <int N>
+__device__ __forceinline__ void cta_allreduce(double (&v)[N], const int (&ops)[N], double (*s_red)[8],
+                                              double *s_out)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const double r = ops[k] == kMax ? warp_max(v[k]) : warp_sum(v[k]);
+        if (lane == 0) s_red[warp][k] = r;
+    }
+    __syncthreads();
+    if (threadIdx.x < N) {
+        const int k = threadIdx.x;
+        double t = s_red[0][k];
+        for (int w = 1; w < kBW; ++w) t = ops[k] == kMax ? fmax(t, s_red[w][k]) : t + s_red[w][k];
+        s_out[k] = t;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = s_out[k];
+}
+
+// y = M x over 32-row warp tiles; f(row, y_row) is called by the lane that
+// owns the row (coalesced over consecutive rows).  A warp reads its tile's
+// entries as one flat, coalesced stream: eight independent index/value loads
+// per lane per 256-entry window, products staged in the warp's scratch, then
+// lane i adds row i's products in order.
+template <class F>
+__device__ __forceinline__ void cta_spmv(const LCsr &M, const double *x, double *scratch, F &&f)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *sc = scratch + warp * kWin;
+    const int ntiles = (M.nrow + 31) >> 5;
+    for (int t = warp; t < ntiles; t += kBW) {
+        const int r0 = t << 5;
+        const int nr = min(32, M.nrow - r0);
+        const int k0 = M.rp[r0], k1 = M.rp[r0 + nr];
+        const int a = lane < nr ? M.rp[r0 + lane] : k1;
+        const int e = lane < nr ? M.rp[r0 + lane + 1] : k1;
+        double mine = 0.0;
+        for (int base = k0; base < k1; base += kWin) {
+            int c[8];
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int k = base + u * 32 + lane;
+                c[u] = k < k1 ? HPR_BATCH_LD(M.ci + k) : 0;
+                v[u] = k < k1 ? HPR_BATCH_LD(M.v + k) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) sc[u * 32 + lane] = v[u] * x[c[u]];
+            __syncwarp();
+            const int lo = max(a, base), hi = min(e, base + kWin);
+            double s0 = 0.0, s1 = 0.0;
+            int j = lo;
+            for (; j + 1 < hi; j += 2) {
+                s0 += sc[j - base];
+                s1 += sc[j + 1 - base];
+            }
+            if (j < hi) s0 += sc[j - base];
+            mine += s0 + s1;
+            __syncwarp();
+        }
+        if (lane < nr) f(r0 + lane, mine);
+    }
+}
+
+// CTA-shared control state of the instance being solved
+struct CtaState {
+    double sigma, lA, lQ;
+    int q_is_diag, noC;
+    int n, m;
+    // restart (HPRQPRestart, include/shared/types.h:177-193)
+    int restart_flag, first_restart;
+    double last_gap, current_gap, save_gap, weighted_norm, best_gap, best_sigma;
+    long long inner, times;
+    // residuals (HPRQPResiduals)
+    double rp, rd, kkt, pobj, dobj, gap;
+    double norm_b_org, norm_c_org, obj_constant;
+    int to_check, do_res, stop, final_status;
+    double red[16];
+    double scal[8];
+};
+
+struct Vecs {
+    double *c, *l, *u, *col_norm, *x, *x_bar, *x_hat, *w, *w_bar, *ATy, *ATy_bar, *ATdy, *Qw, *Qw_bar, *Qx,
+        *dQw, *QATdy, *dx, *dw, *z_bar, *tempv, *diag_Q, *fact1, *fact2, *fact, *fact_M, *last_x, *last_Qw,
+        *last_w, *last_ATy, *fac_c, *pn;
+    double *AL, *AU, *row_norm, *y, *y_bar, *Ax, *dy, *s, *last_y, *fac_r, *pz, *pq;
+};
+
+constexpr int kBatchNVecs = 32, kBatchMVecs = 12;
+
+static __device__ Vecs carve(double *base, int nmax, int mmax, double *smem_pool)
+{
+    Vecs V;
+    double **nv[kBatchNVecs] = {&V.c,      &V.l,      &V.u,      &V.col_norm, &V.x,     &V.x_bar,  &V.x_hat,
+                                &V.w,      &V.w_bar,  &V.ATy,    &V.ATy_bar,  &V.ATdy,  &V.Qw,     &V.Qw_bar,
+                                &V.Qx,     &V.dQw,    &V.QATdy,  &V.dx,       &V.dw,    &V.z_bar,  &V.tempv,
+                                &V.diag_Q, &V.fact1,  &V.fact2,  &V.fact,     &V.fact_M, &V.last_x, &V.last_Qw,
+                                &V.last_w, &V.last_ATy, &V.fac_c, &V.pn};
+    double **mv[kBatchMVecs] = {&V.AL, &V.AU, &V.row_norm, &V.y,     &V.y_bar, &V.Ax,
+                                &V.dy, &V.s,  &V.last_y,   &V.fac_r, &V.pz,    &V.pq};
+    const int na = (nmax + 31) & ~31, ma = (mmax + 31) & ~31;
+    for (int k = 0; k < kBatchNVecs; ++k) *nv[k] = base + (size_t)k * na;
+    for (int k = 0; k < kBatchMVecs; ++k) *mv[k] = base + (size_t)kBatchNVecs * na + (size_t)k * ma;
+    if (smem_pool) {
+        // the gather sources of the step, the residuals and the power iteration
+        V.w = smem_pool;
+        V.w_bar = smem_pool + na;
+        V.tempv = smem_pool + 2 * na;
+        V.x_bar = smem_pool + 3 * na;
+        V.y_bar = smem_pool + 4 * na;
+        V.y = smem_pool + 4 * na + ma;
+    }
+    return V;
+}
+
+__device__ __forceinline__ void scale_rows(const LCsr &M, double *vals, const double *rs, const double *cs)
+{
+    // v *= 1/rs[row]; v /= cs[col]  (reference scale.cu:113-150 roundings)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = warp; r < M.nrow; r += kBW) {
+        const double inv = 1.0 / rs[r];
+        for (int k = M.rp[r] + lane; k < M.rp[r + 1]; k += 32) {
+            double v = vals[k] * inv;
+            v /= cs[M.ci[k]];
+            vals[k] = v;
+        }
+    }
+}
+
+__device__ __forceinline__ double row_abs(const LCsr &M, int r, bool sum)
+{
+    const int lane = threadIdx.x & 31;
+    double acc = 0.0;
+    for (int k = M.rp[r] + lane; k < M.rp[r + 1]; k += 32) {
+        const double a = fabs(M.v[k]);
+        acc = sum ? acc + a : fmax(acc, a);
+    }
+    return sum ? warp_sum(acc) : warp_max(acc);
+}
+
+// Power iteration (reference src/gpu/eigs.cu:185-383), CTA-wide.
+static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q, bool is_a, int len, double *z, double *q,
+                            double *tmp, double *scratch, double (*s_red)[8], double *s_out)
+{
+    if (len == 0) return 0.0;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < len; i += kBT) z[i] = 1.0 + ((double)i + 1.0) / ((double)len + 1.0);
+    double v1[1] = {0.0};
+    const int ops1[1] = {kSum};
+    for (int i = tid; i < len; i += kBT) v1[0] += z[i] * z[i];
+    __syncthreads();
+    cta_allreduce<1>(v1, ops1, s_red, s_out);
+    double zz = v1[0], lambda = 1.0;
+    for (int it = 0; it < 5000; ++it) {
+        const double qn = sqrt(zz);
+        if (qn <= 1e-16) {
+            lambda = 0.0;
+            break;
+        }
+        const double inv = 1.0 / qn;
+        for (int i = tid; i < len; i += kBT) q[i] = z[i] * inv;
+        __syncthreads();
+        double v2[2] = {0.0, 0.0};
+        const int ops2[2] = {kSum, kSum};
+        if (is_a) {
+            cta_spmv(AT, q, scratch, [&](int r, double s) { tmp[r] = s; });
+            __syncthreads();
+            cta_spmv(A, tmp, scratch, [&](int r, double s) {
+                z[r] = s;
+                v2[0] += q[r] * s;
+                v2[1] += s * s;
+            });
+        } else {
+            cta_spmv(Q, q, scratch, [&](int r, double s) {
+                z[r] = s;
+                v2[0] += q[r] * s;
+                v2[1] += s * s;
+            });
+        }
+        __syncthreads();
+        cta_allreduce<2>(v2, ops2, s_red, s_out);
+        lambda = v2[0];
+        zz = v2[1];
+        const double zn = sqrt(zz);
+        double v3[1] = {0.0};
+        for (int i = tid; i < len; i += kBT) {
+            const double r = z[i] - lambda * q[i];
+            q[i] = r;
+            v3[0] += r * r;
+        }
+        __syncthreads();
+        cta_allreduce<1>(v3, ops1, s_red, s_out);
+        if (sqrt(v3[0]) / (zn + fabs(lambda) + 1e-16) < 1e-4) break;
+    }
+    return lambda < 0.0 ? 0.0 : lambda;
+}
+
+static __device__ __forceinline__ size_t adaptive_step_d(long long iter)
+{
+    long long step = 10;
+    if (iter == 0) return step;
+    while (iter / step >= 100) step *= 10;
+    return step;
+}
+
+__global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs B)
+{
+    extern __shared__ __align__(16) double dyn_smem[];
+    double *scratch = dyn_smem;  // kBW * kWin
+    __shared__ CtaState S;
+    __shared__ double s_red[kBW][8];
+    __shared__ double s_out[8];
+    __shared__ int s_inst;
+    const int tid = threadIdx.x;
+    Vecs V = carve(B.ws + (size_t)blockIdx.x * B.ws_stride, B.nmax, B.mmax,
+                   B.vec_smem ? dyn_smem + kBW * kWin : nullptr);
+
+    for (;;) {
+        if (tid == 0) {
+            const int slot = atomicAdd(B.counter, 1);
+            s_inst = slot < B.K ? B.order[slot] : -1;
+        }
+        __syncthreads();
+        const int k = s_inst;
+        __syncthreads();
+        if (k < 0) break;
+        const BInst I = B.inst[k];
+        const int n = I.n, m = I.m;
+        LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz};
+        LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz};
+        LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz};
+        double *qv = B.q_v + I.q_nz, *av = B.a_v + I.a_nz, *atv = B.at_v + I.at_nz;
+        const int q_nnz = Q.rp[n], a_nnz = m > 0 ? A.rp[m] : 0;
+
+        PHASE_T0();
+        const long long _ptot = clock64();
+        // ---- load (scaled copies start as the originals) --------------------
+        for (int i = tid; i < q_nnz; i += kBT) qv[i] = B.q_v0[I.q_nz + i];
+        for (int i = tid; i < a_nnz; i += kBT) {
+            av[i] = B.a_v0[I.a_nz + i];
+            atv[i] = B.at_v0[I.at_nz + i];
+        }
+        for (int i = tid; i < n; i += kBT) {
+            V.c[i] = B.c0[I.var + i];
+            V.l[i] = B.l0[I.var + i];
+            V.u[i] = B.u0[I.var + i];
+            V.col_norm[i] = 1.0;
+        }
+        for (int i = tid; i < m; i += kBT) {
+            V.AL[i] = B.AL0[I.row + i];
+            V.AU[i] = B.AU0[I.row + i];
+            V.row_norm[i] = 1.0;
+        }
+        __syncthreads();
+        // norms of the original data: max bound measure, max |c|
+        {
+            double v[2] = {0.0, 0.0};
+            const int ops[2] = {kMax, kMax};
+            for (int i = tid; i < m; i += kBT) {
+                const double lo = isinf(V.AL[i]) ? 0.0 : fabs(V.AL[i]), hi = isinf(V.AU[i]) ? 0.0 : fabs(V.AU[i]);
+                v[0] = fmax(v[0], lo > hi ? lo : hi);
+            }
+            for (int i = tid; i < n; i += kBT) v[1] = fmax(v[1], fabs(V.c[i]));
+            cta_allreduce<2>(v, ops, s_red, s_out);
+            if (tid == 0) {
+                S.norm_b_org = v[0];
+                S.norm_c_org = v[1];
+            }
+        }
+        // ---- scaling: Ruiz x10 + Pock-Chambolle (reference scale.cu:332-560)
+        if (B.use_scaling) {
+            const int lane = tid & 31, warp = tid >> 5;
+            for (int pass = 0; pass < 11; ++pass) {
+                const bool use_sum = pass == 10;
+                for (int j = warp; j < n; j += kBW) {
+                    double a = m > 0 ? row_abs(AT, j, use_sum) : 0.0;
+                    const double b = row_abs(Q, j, use_sum);
+                    a = use_sum ? a + b : fmax(a, b);
+                    if (lane == 0) V.fac_c[j] = a > 0.0 ? sqrt(a) : 1.0;
+                }
+                for (int r = warp; r < m; r += kBW) {
+                    const double a = row_abs(A, r, use_sum);
+                    if (lane == 0) V.fac_r[r] = a > 0.0 ? sqrt(a) : 1.0;
+                }
+                __syncthreads();
+                scale_rows(Q, qv, V.fac_c, V.fac_c);
+                if (m > 0) {
+                    scale_rows(A, av, V.fac_r, V.fac_c);
+                    scale_rows(AT, atv, V.fac_c, V.fac_r);
+                }
+                for (int i = tid; i < n; i += kBT) {
+                    const double f = V.fac_c[i];
+                    V.col_norm[i] *= f;
+                    V.c[i] /= f;
+                    V.l[i] *= f;
+                    V.u[i] *= f;
+                }
+                for (int i = tid; i < m; i += kBT) {
+                    const double f = V.fac_r[i];
+                    V.row_norm[i] *= f;
+                    V.AL[i] /= f;
+                    V.AU[i] /= f;
+                }
+                __syncthreads();
+            }
+        }
+        PHASE_ADD(0);
+        // ---- setup: sigma0, noC, Q diagonal, eigenvalues (control.cu:156-241)
+        {
+            double v[4] = {0.0, 0.0, 0.0, 0.0};
+            const int ops[4] = {kSum, kSum, kSum, kMax};
+            for (int i = tid; i < m; i += kBT) {
+                const double lo = isinf(V.AL[i]) ? 0.0 : fabs(V.AL[i]), hi = isinf(V.AU[i]) ? 0.0 : fabs(V.AU[i]);
+                const double bm = lo > hi ? lo : hi;
+                v[0] += bm * bm;
+            }
+            for (int i = tid; i < n; i += kBT) {
+                v[1] += V.c[i] * V.c[i];
+                if (isinf(V.l[i]) && isinf(V.u[i])) v[2] += 1.0;
+            }
+            // Q diagonal and largest off-diagonal magnitude
+            const int lane = tid & 31, warp = tid >> 5;
+            double offmax = 0.0, diagmax = 0.0;
+            for (int r = warp; r < n; r += kBW) {
+                double d = 0.0, off = 0.0;
+                for (int kk = Q.rp[r] + lane; kk < Q.rp[r + 1]; kk += 32) {
+                    if (Q.ci[kk] == r) d += Q.v[kk];
+                    else off = fmax(off, fabs(Q.v[kk]));
+                }
+                d = warp_sum(d);
+                off = warp_max(off);
+                if (lane == 0) V.diag_Q[r] = d;
+                offmax = fmax(offmax, off);
+                diagmax = fmax(diagmax, fabs(d));
+            }
+            v[3] = offmax;
+            cta_allreduce<4>(v, ops, s_red, s_out);
+            double v2[1] = {diagmax};
+            const int ops2[1] = {kMax};
+            cta_allreduce<1>(v2, ops2, s_red, s_out);
+            if (tid == 0) {
+                const double nb = sqrt(v[0]), nc = sqrt(v[1]);
+                S.sigma = (nb > 1e-16 && nc > 1e-16 && nb < 1e16 && nc < 1e16) ? nb / nc : 1.0;
+                S.noC = n > 0 && 5.0 * v[2] > 4.0 * (double)n;
+                S.q_is_diag = v[3] <= 1e-15;
+                S.lQ = S.q_is_diag ? v2[0] : 0.0;
+                S.n = n;
+                S.m = m;
+                S.obj_constant = I.obj_constant;
+            }
+            __syncthreads();
+        }
+        PHASE_ADD(1);
+        if (!S.q_is_diag) {
+            const double lq = (q_nnz > 0) ? cta_power(A, AT, Q, false, n, V.pn, V.tempv, V.Qx, scratch, s_red, s_out) : 0.0;
+            if (tid == 0) S.lQ = lq * 1.05;
+        }
+        {
+            const double la = m > 0 ? cta_power(A, AT, Q, true, m, V.pz, V.pq, V.pn, scratch, s_red, s_out) : 0.0;
+            if (tid == 0) S.lA = la * 1.05;
+        }
+        __syncthreads();
+        PHASE_ADD(2);
+        // zero iterates; diagonal factors
+        for (int i = tid; i < n; i += kBT) {
+            V.x[i] = V.x_bar[i] = V.x_hat[i] = V.w[i] = V.w_bar[i] = 0.0;
+            V.ATy[i] = V.ATy_bar[i] = V.ATdy[i] = V.Qw[i] = V.Qw_bar[i] = V.Qx[i] = 0.0;
+            V.dQw[i] = V.QATdy[i] = V.dx[i] = V.dw[i] = V.z_bar[i] = V.tempv[i] = 0.0;
+            V.last_x[i] = V.last_Qw[i] = V.last_w[i] = V.last_ATy[i] = 0.0;
+            if (S.q_is_diag) {
+                const double inv = 1.0 / (1.0 + S.sigma * V.diag_Q[i]);
+                V.fact2[i] = inv;
+                V.fact[i] = S.sigma * inv;
+                V.fact1[i] = S.sigma * V.diag_Q[i] * inv;
+                V.fact_M[i] = S.sigma * S.sigma * inv;
+            }
+        }
+        for (int i = tid; i < m; i += kBT) V.y[i] = V.y_bar[i] = V.Ax[i] = V.dy[i] = V.s[i] = V.last_y[i] = 0.0;
+        if (tid == 0) {
+            S.restart_flag = 0;
+            S.first_restart = 1;
+            S.save_gap = S.current_gap = S.last_gap = S.best_gap = INFINITY;
+            S.weighted_norm = INFINITY;
+            S.best_sigma = S.sigma;
+            S.inner = 0;
+            S.times = 0;
+        }
+        __syncthreads();
+
+        // ---- residuals (reference residuals.cu:81-183) ----------------------
+        auto residuals = [&](long long iter) {
+            if (m > 0) cta_spmv(AT, V.y_bar, scratch, [&](int r, double s) { V.ATdy[r] = s; });
+            else
+                for (int i = tid; i < n; i += kBT) V.ATdy[i] = 0.0;
+            double a[3] = {0.0, 0.0, 0.0};
+            const int opa[3] = {kMax, kMax, kSum};
+            if (m > 0)
+                cta_spmv(A, V.x_bar, scratch, [&](int r, double ax) {
+                    const double proj = clampd(ax, V.AL[r], V.AU[r]);
+                    const double sf = V.row_norm[r];
+                    V.Ax[r] = ax;
+                    V.s[r] = proj;
+                    a[0] = fmax(a[0], fabs((proj - ax) * sf));
+                    a[1] = fmax(a[1], fabs(ax * sf));
+                    a[2] += V.y_bar[r] * proj;
+                });
+            __syncthreads();
+            double q[7] = {0, 0, 0, 0, 0, 0, 0};
+            const int opq[7] = {kMax, kMax, kMax, kSum, kSum, kSum, kMax};
+            cta_spmv(Q, V.x_bar, scratch, [&](int r, double qx) {
+                const double sf = V.col_norm[r];
+                const double xb = V.x_bar[r], aty = V.ATdy[r];
+                V.Qx[r] = qx;
+                const double rd = (qx + V.c[r] - aty - V.z_bar[r]) * sf;
+                q[0] = fmax(q[0], fabs(rd));
+                q[1] = fmax(q[1], fabs(qx * sf));
+                q[2] = fmax(q[2], fabs(aty * sf));
+                q[3] += V.c[r] * xb;
+                q[4] += xb * qx;
+                q[5] += V.z_bar[r] * xb;
+                if (iter == 0) {
+                    const double lo = V.l[r] - xb, hi = xb - V.u[r];
+                    double vv = 0.0;
+                    if (lo > 0.0) vv += lo;
+                    if (hi > 0.0) vv += hi;
+                    q[6] = fmax(q[6], fabs(vv * (1.0 / sf)));
+                }
+            });
+            cta_allreduce<3>(a, opa, s_red, s_out);
+            cta_allreduce<7>(q, opq, s_red, s_out);
+            if (tid == 0) {
+                S.pobj = (q[3] + 0.5 * q[4]) + S.obj_constant;
+                S.dobj = (-0.5 * q[4] + q[5] + a[2]) + S.obj_constant;
+                S.gap = fabs(S.pobj - S.dobj) / (1.0 + fmax(fabs(S.pobj), fabs(S.dobj)));
+                S.rd = q[0] / (1.0 + fmax(S.norm_c_org, fmax(q[2], q[1])));
+                S.rp = m > 0 ? a[0] / (1.0 + fmax(S.norm_b_org, a[1])) : 0.0;
+                if (iter == 0 && q[6] > S.rp) S.rp = q[6];
+                S.kkt = fmax(S.rp, fmax(S.rd, S.gap));
+            }
+            __syncthreads();
+        };
+
+        // ---- one HPR step (reference iteration.cu:1386-1442) ------------------
+        auto step = [&](int full) {
+            const double sigma = S.sigma, lA = S.lA, lQ = S.lQ;
+            const double h1 = 1.0 / ((double)S.inner + 2.0), h2 = 1.0 - h1;
+            const double f2s = 1.0 / (1.0 + sigma * lQ), f1s = 1.0 - f2s;
+            const int diag = S.q_is_diag;
+            if (S.noC) {
+                auto upd = [&](int i, double aty) {
+                    const double xi = V.x[i], wi = V.w[i];
+                    V.ATy[i] = aty;
+                    const double z_raw = xi + sigma * (-V.Qw[i] + aty - V.c[i]);
+                    const double xb = clampd(z_raw, V.l[i], V.u[i]);
+                    const double xh = 2.0 * xb - xi;
+                    const double wb = diag ? V.fact1[i] * wi + V.fact2[i] * xh : f1s * wi + f2s * xh;
+                    if (full) {
+                        V.x_bar[i] = xb;
+                        V.z_bar[i] = (xb - z_raw) / sigma;
+                        V.dx[i] = xb - xi;
+                        V.dw[i] = wb - wi;
+                    }
+                    V.x_hat[i] = xh;
+                    V.x[i] = h2 * xh + h1 * V.last_x[i];
+                    V.w_bar[i] = wb;
+                    V.w[i] = h2 * (2.0 * wb - wi) + h1 * V.last_w[i];
+                };
+                if (m > 0) cta_spmv(AT, V.y, scratch, upd);
+                else
+                    for (int i = tid; i < n; i += kBT) upd(i, 0.0);
+                __syncthreads();
+                cta_spmv(Q, V.w_bar, scratch, [&](int i, double qwb) {
+                    const double qw = V.Qw[i];
+                    V.Qw_bar[i] = qwb;
+                    V.Qw[i] = h2 * (2.0 * qwb - qw) + h1 * V.last_Qw[i];
+                    V.tempv[i] = V.x_hat[i] + sigma * (qw - qwb);
+                });
+                __syncthreads();
+            } else {
+                cta_spmv(Q, V.w, scratch, [&](int i, double qw) {
+                    const double xi = V.x[i], wi = V.w[i];
+                    const double z_raw = xi + sigma * (-qw + V.ATy[i] - V.c[i]);
+                    const double xb = clampd(z_raw, V.l[i], V.u[i]);
+                    const double xh = 2.0 * xb - xi;
+                    V.Qw[i] = qw;
+                    V.x_hat[i] = xh;
+                    if (full) {
+                        V.x_bar[i] = xb;
+                        V.z_bar[i] = (xb - z_raw) / sigma;
+                        V.dx[i] = xb - xi;
+                    }
+                    V.x[i] = h2 * xh + h1 * V.last_x[i];
+                    V.w_bar[i] = diag ? V.fact1[i] * wi + V.fact2[i] * xh : f1s * wi + f2s * xh;
+                });
+                __syncthreads();
+                if (m > 0) {
+                    cta_spmv(Q, V.w_bar, scratch,
+                             [&](int i, double qwb) { V.tempv[i] = V.x_hat[i] + sigma * (V.Qw[i] - qwb); });
+                    __syncthreads();
+                }
+            }
+            if (m > 0) {
+                const double f1 = lA * sigma, f2 = 1.0 / f1;
+                cta_spmv(A, V.tempv, scratch, [&](int i, double ax) {
+                    const double yi = V.y[i];
+                    const double s_raw = ax - f1 * yi;
+                    const double sp = clampd(s_raw, V.AL[i], V.AU[i]);
+                    const double yb = f2 * (sp - s_raw);
+                    V.y_bar[i] = yb;
+                    if (full) {
+                        V.Ax[i] = ax;
+                        V.dy[i] = yb - yi;
+                        V.s[i] = sp;
+                    }
+                    V.y[i] = h2 * (2.0 * yb - yi) + h1 * V.last_y[i];
+                });
+                __syncthreads();
+            }
+            if (!S.noC) {
+                const double fs = sigma / (1.0 + sigma * lQ);
+                auto w2 = [&](int i, double atyb) {
+                    const double f = diag ? V.fact[i] : fs;
+                    const double aty = V.ATy[i], wi = V.w[i];
+                    const double wbn = V.w_bar[i] + f * (atyb - aty);
+                    if (full) {
+                        V.dw[i] = wbn - wi;
+                        V.ATdy[i] = atyb - aty;
+                        V.w_bar[i] = wbn;
+                        V.ATy_bar[i] = atyb;
+                    }
+                    V.w[i] = h1 * V.last_w[i] + h2 * (2.0 * wbn - wi);
+                    V.ATy[i] = h1 * V.last_ATy[i] + h2 * (2.0 * atyb - aty);
+                };
+                if (m > 0) cta_spmv(AT, V.y_bar, scratch, w2);
+                else
+                    for (int i = tid; i < n; i += kBT) w2(i, 0.0);
+                __syncthreads();
+            }
+        };
+
+        // ---- M-norm (reference control.cu:243-332) ---------------------------
+        auto m_norm = [&]() -> double {
+            double a[4] = {0, 0, 0, 0};
+            const int ops4[4] = {kSum, kSum, kSum, kSum};
+            cta_spmv(Q, V.dw, scratch, [&](int i, double v) {
+                V.dQw[i] = v;
+                const double dx = V.dx[i];
+                a[0] += dx * dx;
+                a[1] += v * dx;
+                a[2] += v * v;
+                a[3] += V.dw[i] * v;
+            });
+            __syncthreads();
+            double b[2] = {0, 0}, c3[3] = {0, 0, 0};
+            const int ops2[2] = {kSum, kSum}, ops3[3] = {kSum, kSum, kSum};
+            if (m > 0) {
+                cta_spmv(AT, V.dy, scratch, [&](int i, double v) {
+                    V.ATdy[i] = v;
+                    b[0] += v * V.dx[i];
+                });
+                for (int i = tid; i < m; i += kBT) b[1] += V.dy[i] * V.dy[i];
+                __syncthreads();
+                cta_spmv(Q, V.ATdy, scratch, [&](int i, double v) {
+                    V.QATdy[i] = v;
+                    const double at = V.ATdy[i];
+                    c3[0] += V.dQw[i] * at;
+                    c3[1] += at * v;
+                    if (S.q_is_diag) c3[2] += (at * V.fact_M[i]) * v;
+                });
+            }
+            cta_allreduce<4>(a, ops4, s_red, s_out);
+            cta_allreduce<2>(b, ops2, s_red, s_out);
+            cta_allreduce<3>(c3, ops3, s_red, s_out);
+            const double sigma = S.sigma, lA = S.lA, lQ = S.lQ;
+            double m1 = 0.0, m3 = 0.0, m2 = (1.0 / sigma) * a[0];
+            m2 -= 2.0 * a[1];
+            if (m > 0) {
+                m1 = sigma * lA * b[1];
+                m1 -= 2.0 * sigma * c3[0];
+                m2 += 2.0 * b[0];
+                if (S.q_is_diag) {
+                    m3 = c3[2];
+                    m1 += sigma * a[2];
+                } else {
+                    m3 = (sigma * sigma) / (1.0 + sigma * lQ) * c3[1];
+                    m1 += sigma * lQ * a[3];
+                }
+            } else if (!S.q_is_diag) {
+                m1 = sigma * lQ * a[3];
+            }
+            m2 += m1 > 0.0 ? m1 : 0.0;
+            return sqrt((m2 > 0.0 ? m2 : 0.0) + (m3 > 0.0 ? m3 : 0.0));
+        };
+
+        // ---- sigma update (reference control.cu:334-529) ----------------------
+        auto sigma_update = [&]() {
+            const double sigma_old = S.sigma, lA = S.lA, lQ = S.lQ;
+            double d[2] = {0, 0};
+            const int ops2[2] = {kSum, kSum};
+            for (int i = tid; i < n; i += kBT) {
+                const double dx = V.x_bar[i] - V.last_x[i];
+                V.dx[i] = dx;
+                V.dw[i] = V.w_bar[i] - V.last_w[i];
+                d[0] += dx * dx;
+                if (m > 0) V.ATdy[i] = V.ATy_bar[i] - V.last_ATy[i];
+            }
+            for (int i = tid; i < m; i += kBT) {
+                const double dy = V.y_bar[i] - V.last_y[i];
+                V.dy[i] = dy;
+                d[1] += dy * dy;
+            }
+            __syncthreads();
+            double e3[3] = {0, 0, 0}, f1v[1] = {0};
+            const int ops3[3] = {kSum, kSum, kSum}, ops1[1] = {kSum};
+            cta_spmv(Q, V.dw, scratch, [&](int i, double v) {
+                V.dQw[i] = v;
+                if (m > 0) e3[0] += v * V.ATdy[i];
+                e3[1] += v * v;
+                e3[2] += V.dw[i] * v;
+            });
+            if (m > 0) {
+                cta_spmv(Q, V.ATdy, scratch, [&](int i, double v) {
+                    V.QATdy[i] = v;
+                    f1v[0] += V.ATdy[i] * v;
+                });
+            }
+            cta_allreduce<2>(d, ops2, s_red, s_out);
+            cta_allreduce<3>(e3, ops3, s_red, s_out);
+            cta_allreduce<1>(f1v, ops1, s_red, s_out);
+            double a = 0.0, b = d[0], c_term = 0.0, d_term = 0.0;
+            if (m > 0) a = lA * d[1] - 2.0 * e3[0];
+            if (S.q_is_diag) {
+                a += e3[1];
+            } else {
+                a += lQ * e3[2];
+                if (m > 0) {
+                    c_term = f1v[0];
+                    d_term = lQ;
+                }
+            }
+            a = fmax(a, 1e-12);
+            b = fmax(b, 1e-12);
+            double est;
+            if (S.q_is_diag && m > 0) {
+                // golden section with a CTA-wide sum per probe
+                double left = 1e-12, right = 1e12;
+                const double phi = (sqrt(5.0) - 1.0) / 2.0;
+                auto f = [&](double xp) {
+                    double t[1] = {0.0};
+                    for (int i = tid; i < n; i += kBT) t[0] += V.ATdy[i] * (V.QATdy[i] / (1.0 + xp * V.diag_Q[i]));
+                    cta_allreduce<1>(t, ops1, s_red, s_out);
+                    return a * xp + b / xp + xp * xp * t[0];
+                };
+                double x1 = right - phi * (right - left), x2 = left + phi * (right - left);
+                double fa = f(x1), fb = f(x2);
+                for (int it = 0; it < 200; ++it) {
+                    if (fabs(right - left) <= 1e-12 * fmax(1.0, fabs(left))) break;
+                    if (fa > fb) {
+                        left = x1;
+                        x1 = x2;
+                        fa = fb;
+                        x2 = left + phi * (right - left);
+                        fb = f(x2);
+                    } else {
+                        right = x2;
+                        x2 = x1;
+                        fb = fa;
+                        x1 = right - phi * (right - left);
+                        fa = f(x1);
+                    }
+                }
+                est = fa < fb ? x1 : x2;
+            } else if (!S.q_is_diag && m > 0) {
+                const double cc = c_term > 0.0 ? c_term : 0.0, dd = d_term > 0.0 ? d_term : 0.0;
+                double left = 1e-12, right = 1e12;
+                const double ip = (sqrt(5.0) - 1.0) / 2.0, ip2 = (3.0 - sqrt(5.0)) / 2.0;
+                auto f = [&](double xp) { return a * xp + b / xp + cc * xp * xp / (1.0 + dd * xp); };
+                double x1 = left + ip2 * (right - left), x2 = left + ip * (right - left);
+                double fa = f(x1), fb = f(x2);
+                for (int it = 0; it < 256; ++it) {
+                    if (fabs(right - left) <= 1e-13 * fmax(1.0, fmax(fabs(left), fabs(right)))) break;
+                    if (fa > fb) {
+                        left = x1;
+                        x1 = x2;
+                        fa = fb;
+                        x2 = left + ip * (right - left);
+                        fb = f(x2);
+                    } else {
+                        right = x2;
+                        x2 = x1;
+                        fb = fa;
+                        x1 = left + ip2 * (right - left);
+                        fa = f(x1);
+                    }
+                }
+                est = 0.5 * (left + right);
+            } else {
+                est = sqrt(b / a);
+            }
+            if (tid == 0) {
+                est = clampd(est, 1e-12, 1e12);
+                const double fact =
+                    (S.best_gap > 0.0 && isfinite(S.best_gap)) ? exp(-0.05 * (S.current_gap / S.best_gap)) : 1.0;
+                const double cand =
+                    exp(fact * log(est) + (1.0 - fact) * log(S.best_sigma > 0.0 ? S.best_sigma : sigma_old));
+                double kappa = 1.0;
+                const double t1 = fmax(fmin(S.rd, S.rp), fmin(S.gap, S.current_gap));
+                if (t1 <= 9e-10 && S.rp > 0.0) {
+                    const double ratio = S.rd / S.rp;
+                    kappa = t1 > 5e-10 ? clampd(sqrt(ratio), 1e-2, 100.0) : clampd(ratio, 1e-2, 100.0);
+                }
+                S.sigma = clampd(kappa * cand, 1e-12, 1e12);
+                S.scal[0] = sigma_old;
+            }
+            __syncthreads();
+            if (S.q_is_diag && fabs(S.sigma - S.scal[0]) > 1e-15) {
+                const double sg = S.sigma;
+                for (int i = tid; i < n; i += kBT) {
+                    const double inv = 1.0 / (1.0 + sg * V.diag_Q[i]);
+                    V.fact2[i] = inv;
+                    V.fact[i] = sg * inv;
+                    V.fact1[i] = sg * V.diag_Q[i] * inv;
+                    V.fact_M[i] = sg * sg * inv;
+                }
+                __syncthreads();
+            }
+        };
+
+        auto restart_apply = [&]() {
+            for (int i = tid; i < n; i += kBT) {
+                const double xb = V.x_bar[i], wb = V.w_bar[i];
+                V.x[i] = V.last_x[i] = xb;
+                V.w[i] = V.last_w[i] = wb;
+                if (S.noC) V.Qw[i] = V.last_Qw[i] = V.Qw_bar[i];
+            }
+            for (int i = tid; i < m; i += kBT) V.y[i] = V.last_y[i] = V.y_bar[i];
+            if (m > 0) {
+                cta_spmv(AT, V.y_bar, scratch, [&](int i, double s) { V.ATy_bar[i] = V.ATy[i] = V.last_ATy[i] = s; });
+            }
+            __syncthreads();
+            if (tid == 0) {
+                S.last_gap = S.current_gap;
+                S.save_gap = INFINITY;
+                S.times += 1;
+                S.inner = 0;
+            }
+            __syncthreads();
+        };
+
+        // ---- outer loop (reference solver_backend.c:432-513) ------------------
+        residuals(0);
+        long long iter;
+        for (iter = 0;; ++iter) {
+            if (tid == 0) {
+                const double el = 1e-9 * (double)(globaltimer_ns() - B.t_start);
+                int print_yes = 0;
+                if (iter > 0) {
+                    if (B.print_frequency == -1 &&
+                        ((long long)(iter % (long long)adaptive_step_d(iter)) == 0 || iter == B.max_iter ||
+                         el > B.time_limit))
+                        print_yes = 1;
+                    if (B.print_frequency > 0 &&
+                        (iter % B.print_frequency == 0 || iter == B.max_iter || el > B.time_limit))
+                        print_yes = 1;
+                }
+                S.do_res = iter > 0 && ((B.check_iter > 0 && iter % B.check_iter == 0) || print_yes);
+                S.scal[1] = el;
+            }
+            __syncthreads();
+            PHASE_ADD(3);
+            if (S.do_res) residuals(iter);
+            PHASE_ADD(4);
+            if (tid == 0) {
+                const double el = S.scal[1];
+                int fs;
+                if (S.kkt < B.stoptol) fs = 6;
+                else if (iter == B.max_iter) fs = 4;
+                else if (el > B.time_limit) fs = 5;
+                else fs = 7;
+                S.final_status = fs;
+                // restart_check (src/cpu/control.c:231-282)
+                const long long ci = B.check_iter;
+                if (ci > 0) {
+                    S.restart_flag = 0;
+                    if (S.first_restart) {
+                        if (iter == ci) {
+                            S.first_restart = 0;
+                            S.restart_flag = 1;
+                            S.weighted_norm = S.current_gap;
+                            S.best_gap = S.current_gap;
+                            S.best_sigma = S.sigma;
+                        }
+                    } else if (iter % ci == 0) {
+                        if (S.current_gap < 0.0) S.current_gap = 1e-6;
+                        if (S.current_gap <= 0.2 * S.last_gap) S.restart_flag = 1;
+                        if (S.current_gap <= 0.8 * S.last_gap && S.current_gap > S.save_gap) S.restart_flag = 2;
+                        const double f =
+                            (S.weighted_norm > 0.0 && S.current_gap / S.weighted_norm > 1e-1) ? 0.5 : 0.2;
+                        if ((double)S.inner >= f * (double)iter) S.restart_flag = 3;
+                        if (S.best_gap > S.current_gap) {
+                            S.best_gap = S.current_gap;
+                            S.best_sigma = S.sigma;
+                        }
+                        S.save_gap = S.current_gap;
+                    }
+                }
+            }
+            __syncthreads();
+            if (S.restart_flag > 0) {
+                sigma_update();
+                restart_apply();
+            }
+            PHASE_ADD(6);
+            if (S.final_status != 7) break;
+            if (tid == 0) {
+                const long long nx = iter + 1;
+                int t = 0;
+                if (B.check_iter > 0 && nx % B.check_iter == 0) t = 1;
+                if (S.restart_flag > 0) t = 1;
+                if (B.print_frequency == -1 && nx % (long long)adaptive_step_d(nx) == 0) t = 1;
+                if (B.print_frequency > 0 && nx % B.print_frequency == 0) t = 1;
+                S.to_check = t;
+            }
+            __syncthreads();
+            step(S.to_check);
+            PHASE_ADD(3);
+            const bool at_check = B.check_iter > 0 && (iter + 1) % B.check_iter == 0;
+            if (S.restart_flag > 0 || at_check) {
+                const double g = m_norm();
+                if (tid == 0) {
+                    if (S.restart_flag > 0) S.last_gap = g;
+                    if (at_check) S.current_gap = g;
+                    if (!isfinite(g)) S.final_status = 1;
+                }
+                __syncthreads();
+                PHASE_ADD(5);
+                if (S.final_status == 1) break;
+            }
+            if (tid == 0) S.inner += 1;
+            __syncthreads();
+        }
+
+        // ---- output (reference workspace.cu:427-511) ---------------------------
+        for (int i = tid; i < n; i += kBT) {
+            const double cn = V.col_norm[i];
+            B.x[I.var + i] = V.x_bar[i] / cn;
+            B.w[I.var + i] = V.w_bar[i] / cn;
+            B.z[I.var + i] = V.z_bar[i] * cn;
+            if (B.active_x) B.active_x[I.var + i] = V.z_bar[i] != 0.0;
+        }
+        for (int i = tid; i < m; i += kBT) {
+            B.y[I.row + i] = V.y_bar[i] / V.row_norm[i];
+            if (B.active_r) B.active_r[I.row + i] = V.y_bar[i] != 0.0;
+        }
+        if (B.phase_clk && tid == 0) B.phase_clk[blockIdx.x * 8 + 7] += (unsigned long long)(clock64() - _ptot);
+        if (tid == 0) {
+            B.status[k] = S.final_status;
+            B.iters[k] = iter;
+            B.pobj[k] = S.pobj;
+            B.resid[k] = S.kkt;
+            B.gap[k] = S.gap;
+            B.restarts[k] = (int)S.times;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_batch_clock(unsigned long long *t)
+{
+    *t = globaltimer_ns();
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+#define B_CK(call)                                                                                     \
+    do {                                                                                               \
+        cudaError_t err__ = (call);                                                                    \
+        if (err__ != cudaSuccess) {                                                                    \
+            fprintf(stderr, "hprqp-b200 batch: CUDA error %s at %s:%d\n", cudaGetErrorString(err__), __FILE__, \
+                    __LINE__);                                                                         \
+            return HPRQP_STATUS_NOT_IMPLEMENTED;                                                       \
+        }                                                                                              \
+    } while (0)
+
+}  // namespace hpr
+
+struct HPRQPBatch {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    size_t K = 0;
+    std::vector<size_t> var_off, row_off;          // original packing (caller's layout)
+    std::vector<int> n_k, m_k;                      // preprocessed sizes
+    std::vector<std::vector<size_t>> kept_rows;     // per instance: original local row of each kept row
+    std::vector<hpr::BInst> inst;
+    size_t total_n = 0, total_m = 0, total_m_orig = 0;
+    int nmax = 0, mmax = 0;
+    std::vector<void *> allocs;
+    hpr::BatchArgs args{};
+    double last_ms = 0.0;
+    bool solved = false;
+    // host copies of the preprocessed models (kept for the adjoint)
+    std::vector<HPRQPModel> models;
+};
+
+namespace hpr {
+
+template <class T>
+static HPRQPStatus balloc(HPRQPBatch *b, T **p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    void *ptr = nullptr;
+    if (cudaMalloc(&ptr, count * sizeof(T)) != cudaSuccess) {
+        fprintf(stderr, "hprqp-b200 batch: cudaMalloc(%zu bytes) failed\n", count * sizeof(T));
+        return HPRQP_STATUS_ALLOCATION_FAILED;
+    }
+    b->allocs.push_back(ptr);
+    *p = (T *)ptr;
+    return HPRQP_STATUS_OK;
+}
+
+static void batch_free(HPRQPBatch *b)
+{
+    for (void *p : b->allocs) cudaFree(p);
+    b->allocs.clear();
+    for (auto &m : b->models) model_free(&m);
+    b->models.clear();
+    if (b->stream) cudaStreamDestroy(b->stream);
+    b->stream = nullptr;
+}
+
+// extract instance k of a block-diagonal CSR (rows [r0, r1), columns
+// [c0, c1)) as a local CSR view into freshly allocated arrays
+static HPRQPStatus extract_block(const HPRQPMatrixCSR *M, size_t r0, size_t r1, size_t c0, size_t c1,
+                                 std::vector<size_t> &rp, std::vector<size_t> &ci, std::vector<double> &v)
+{
+    rp.assign(r1 - r0 + 1, 0);
+    ci.clear();
+    v.clear();
+    for (size_t r = r0; r < r1; ++r) {
+        for (size_t k = M->row_ptr[r]; k < M->row_ptr[r + 1]; ++k) {
+            const size_t c = M->col_ind[k];
+            if (c < c0 || c >= c1) return HPRQP_STATUS_INVALID_ARGUMENT;  // not block diagonal
+            ci.push_back(c - c0);
+            v.push_back(M->values[k]);
+        }
+        rp[r - r0 + 1] = ci.size();
+    }
+    return HPRQP_STATUS_OK;
+}
+
+}  // namespace hpr
+
+extern "C" {
+
+void hprqp_batch_params_set_defaults(HPRQPBatchParams *p)
+{
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->stoptol = 1e-6;
+    p->max_iter = (size_t)INT_MAX;
+    p->time_limit = 3600.0;
+    p->check_iter = 100;
+    p->print_frequency = -1;
+    p->use_scaling = 1;
+    p->device_number = 0;
+}
+
+HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t *row_offsets,
+                               const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c, const double *AL,
+                               const double *AU, const double *l, const double *u, const double *obj_constants,
+                               int device_number, HPRQPBatch **out)
+{
+    using namespace hpr;
+    if (!out || !var_offsets || !row_offsets || !Q || !A || !c || !l || !u || K == 0)
+        return HPRQP_STATUS_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!matrix_csr_is_valid(Q) || !matrix_csr_is_valid(A) || Q->nrow != Q->ncol || A->ncol != Q->ncol ||
+        var_offsets[0] != 0 || row_offsets[0] != 0 || var_offsets[K] != Q->nrow || row_offsets[K] != A->nrow)
+        return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (A->nrow > 0 && (!AL || !AU)) return HPRQP_STATUS_INVALID_ARGUMENT;
+    for (size_t k = 0; k < K; ++k)
+        if (var_offsets[k + 1] < var_offsets[k] || row_offsets[k + 1] < row_offsets[k])
+            return HPRQP_STATUS_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        fprintf(stderr, "hprqp-b200: no CUDA device available; this engine has no CPU fallback\n");
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
+    }
+    if (device_number < 0 || device_number >= ndev) return HPRQP_STATUS_INVALID_ARGUMENT;
+
+    HPRQPBatch *b = new HPRQPBatch();
+    b->K = K;
+    b->device = device_number;
+    b->var_off.assign(var_offsets, var_offsets + K + 1);
+    b->row_off.assign(row_offsets, row_offsets + K + 1);
+    b->total_m_orig = A->nrow;
+    b->models.resize(K);
+    for (auto &mm : b->models) model_init(&mm);
+    b->kept_rows.resize(K);
+    // ---- per-instance build + preprocess (the single-QP builder), threaded
+    std::vector<HPRQPStatus> st_k(K, HPRQP_STATUS_OK);
+    const unsigned nth = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    auto worker = [&](unsigned tix) {
+        std::vector<size_t> qrp, qci, arp, aci;
+        std::vector<double> qv, av;
+        for (size_t k = tix; k < K; k += nth) {
+            const size_t v0 = var_offsets[k], v1 = var_offsets[k + 1], r0 = row_offsets[k], r1 = row_offsets[k + 1];
+            HPRQPStatus st = extract_block(Q, v0, v1, v0, v1, qrp, qci, qv);
+            if (st == HPRQP_STATUS_OK) st = extract_block(A, r0, r1, v0, v1, arp, aci, av);
+            if (st != HPRQP_STATUS_OK) {
+                st_k[k] = st;
+                continue;
+            }
+            size_t e_idx = 0;
+            double e_val = 0.0;
+            HPRQPMatrixCSR q{v1 - v0, v1 - v0, qci.size(), qrp.data(), qci.empty() ? &e_idx : qci.data(),
+                             qv.empty() ? &e_val : qv.data(), 0};
+            HPRQPMatrixCSR a{r1 - r0, v1 - v0, aci.size(), arp.data(), aci.empty() ? &e_idx : aci.data(),
+                             av.empty() ? &e_val : av.data(), 0};
+            st = build_from_QAbc(&q, &a, c + v0, r1 > r0 ? AL + r0 : nullptr, r1 > r0 ? AU + r0 : nullptr, l + v0,
+                                 u + v0, obj_constants ? obj_constants[k] : 0.0, &b->models[k]);
+            st_k[k] = st;
+            if (st == HPRQP_STATUS_OK) {
+                // record which original rows survived preprocessing
+                auto &kr = b->kept_rows[k];
+                kr.clear();
+                for (size_t r = r0; r < r1; ++r) {
+                    const size_t len = A->row_ptr[r + 1] - A->row_ptr[r];
+                    const bool free_row = std::isinf(AL[r]) && AL[r] < 0 && std::isinf(AU[r]) && AU[r] > 0;
+                    if (len > 0 && !free_row) kr.push_back(r - r0);
+                }
+            }
+        }
+    };
+    {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nth; ++t) th.emplace_back(worker, t);
+        for (auto &t : th) t.join();
+    }
+    for (size_t k = 0; k < K; ++k)
+        if (st_k[k] != HPRQP_STATUS_OK) {
+            HPRQPStatus st = st_k[k];
+            batch_free(b);
+            delete b;
+            return st;
+        }
+    // ---- pack (int32 local indices)
+    size_t qnz = 0, anz = 0, qrp = 0, arp = 0, atrp = 0, nv = 0, nr = 0;
+    b->inst.resize(K);
+    for (size_t k = 0; k < K; ++k) {
+        const HPRQPModel &M = b->models[k];
+        BInst &I = b->inst[k];
+        I.q_nz = (long long)qnz;
+        I.a_nz = (long long)anz;
+        I.at_nz = (long long)anz;
+        I.q_rp = (int)qrp;
+        I.a_rp = (int)arp;
+        I.at_rp = (int)atrp;
+        I.var = (int)nv;
+        I.row = (int)nr;
+        I.n = (int)M.Q.ncol;
+        I.m = (int)M.A.nrow;
+        I.obj_constant = M.obj_constant;
+        qnz += M.Q.nnz;
+        anz += M.A.nnz;
+        qrp += M.Q.nrow + 1;
+        arp += M.A.nrow + 1;
+        atrp += M.AT.nrow + 1;
+        nv += M.Q.ncol;
+        nr += M.A.nrow;
+        b->nmax = std::max(b->nmax, I.n);
+        b->mmax = std::max(b->mmax, I.m);
+    }
+    if (qrp > (size_t)INT32_MAX || arp > (size_t)INT32_MAX || nv > (size_t)INT32_MAX || nr > (size_t)INT32_MAX) {
+        batch_free(b);
+        delete b;
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
+    }
+    b->total_n = nv;
+    b->total_m = nr;
+    std::vector<int> h_qrp(qrp), h_arp(arp), h_atrp(atrp), h_qci(std::max<size_t>(qnz, 1)),
+        h_aci(std::max<size_t>(anz, 1)), h_atci(std::max<size_t>(anz, 1));
+    std::vector<double> h_qv(std::max<size_t>(qnz, 1)), h_av(std::max<size_t>(anz, 1)), h_atv(std::max<size_t>(anz, 1)),
+        h_c(std::max<size_t>(nv, 1)), h_l(std::max<size_t>(nv, 1)), h_u(std::max<size_t>(nv, 1)),
+        h_AL(std::max<size_t>(nr, 1)), h_AU(std::max<size_t>(nr, 1));
+    for (size_t k = 0; k < K; ++k) {
+        const HPRQPModel &M = b->models[k];
+        const BInst &I = b->inst[k];
+        for (size_t r = 0; r <= M.Q.nrow; ++r) h_qrp[I.q_rp + r] = (int)M.Q.row_ptr[r];
+        for (size_t r = 0; r <= M.A.nrow; ++r) h_arp[I.a_rp + r] = (int)M.A.row_ptr[r];
+        for (size_t r = 0; r <= M.AT.nrow; ++r) h_atrp[I.at_rp + r] = (int)M.AT.row_ptr[r];
+        for (size_t e = 0; e < M.Q.nnz; ++e) {
+            h_qci[I.q_nz + e] = (int)M.Q.col_ind[e];
+            h_qv[I.q_nz + e] = M.Q.values[e];
+        }
+        for (size_t e = 0; e < M.A.nnz; ++e) {
+            h_aci[I.a_nz + e] = (int)M.A.col_ind[e];
+            h_av[I.a_nz + e] = M.A.values[e];
+            h_atci[I.at_nz + e] = (int)M.AT.col_ind[e];
+            h_atv[I.at_nz + e] = M.AT.values[e];
+        }
+        memcpy(&h_c[I.var], M.c, M.Q.ncol * sizeof(double));
+        memcpy(&h_l[I.var], M.l, M.Q.ncol * sizeof(double));
+        memcpy(&h_u[I.var], M.u, M.Q.ncol * sizeof(double));
+        if (M.A.nrow) {
+            memcpy(&h_AL[I.row], M.AL, M.A.nrow * sizeof(double));
+            memcpy(&h_AU[I.row], M.AU, M.A.nrow * sizeof(double));
+        }
+    }
+    // ---- device
+    HPRQPStatus st = HPRQP_STATUS_OK;
+    auto fail = [&](HPRQPStatus s) {
+        batch_free(b);
+        delete b;
+        return s;
+    };
+    if (cudaSetDevice(device_number) != cudaSuccess ||
+        cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device_number) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
+    BatchArgs &G = b->args;
+    G.K = (int)K;
+    int *d_qrp, *d_arp, *d_atrp, *d_qci, *d_aci, *d_atci;
+    double *d_qv0, *d_av0, *d_atv0, *d_c, *d_l, *d_u, *d_AL, *d_AU;
+    BInst *d_inst;
+    int *d_order, *d_counter;
+    if ((st = balloc(b, &d_qrp, qrp)) || (st = balloc(b, &d_arp, arp)) || (st = balloc(b, &d_atrp, atrp)) ||
+        (st = balloc(b, &d_qci, h_qci.size())) || (st = balloc(b, &d_aci, h_aci.size())) ||
+        (st = balloc(b, &d_atci, h_atci.size())) || (st = balloc(b, &d_qv0, h_qv.size())) ||
+        (st = balloc(b, &d_av0, h_av.size())) || (st = balloc(b, &d_atv0, h_atv.size())) ||
+        (st = balloc(b, &G.q_v, h_qv.size())) || (st = balloc(b, &G.a_v, h_av.size())) ||
+        (st = balloc(b, &G.at_v, h_atv.size())) || (st = balloc(b, &d_c, h_c.size())) ||
+        (st = balloc(b, &d_l, h_l.size())) || (st = balloc(b, &d_u, h_u.size())) ||
+        (st = balloc(b, &d_AL, h_AL.size())) || (st = balloc(b, &d_AU, h_AU.size())) ||
+        (st = balloc(b, &d_inst, K)) || (st = balloc(b, &d_order, K)) || (st = balloc(b, &d_counter, 1)) ||
+        (st = balloc(b, &G.x, h_c.size())) || (st = balloc(b, &G.z, h_c.size())) || (st = balloc(b, &G.w, h_c.size())) ||
+        (st = balloc(b, &G.y, h_AL.size())) || (st = balloc(b, &G.status, K)) || (st = balloc(b, &G.iters, K)) ||
+        (st = balloc(b, &G.pobj, K)) || (st = balloc(b, &G.resid, K)) || (st = balloc(b, &G.gap, K)) ||
+        (st = balloc(b, &G.restarts, K)) || (st = balloc(b, &G.active_x, h_c.size())) ||
+        (st = balloc(b, &G.active_r, h_AL.size())))
+        return fail(st);
+    // largest instances first
+    std::vector<int> order(K);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const long long wx = b->models[x].Q.nnz + 2 * b->models[x].A.nnz + b->models[x].Q.ncol;
+        const long long wy = b->models[y].Q.nnz + 2 * b->models[y].A.nnz + b->models[y].Q.ncol;
+        return wx > wy;
+    });
+    auto up = [&](void *d, const void *h, size_t bytes) {
+        return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, b->stream) == cudaSuccess;
+    };
+    if (!up(d_qrp, h_qrp.data(), qrp * 4) || !up(d_arp, h_arp.data(), arp * 4) || !up(d_atrp, h_atrp.data(), atrp * 4) ||
+        !up(d_qci, h_qci.data(), h_qci.size() * 4) || !up(d_aci, h_aci.data(), h_aci.size() * 4) ||
+        !up(d_atci, h_atci.data(), h_atci.size() * 4) || !up(d_qv0, h_qv.data(), h_qv.size() * 8) ||
+        !up(d_av0, h_av.data(), h_av.size() * 8) || !up(d_atv0, h_atv.data(), h_atv.size() * 8) ||
+        !up(d_c, h_c.data(), h_c.size() * 8) || !up(d_l, h_l.data(), h_l.size() * 8) ||
+        !up(d_u, h_u.data(), h_u.size() * 8) || !up(d_AL, h_AL.data(), h_AL.size() * 8) ||
+        !up(d_AU, h_AU.data(), h_AU.size() * 8) || !up(d_inst, b->inst.data(), K * sizeof(BInst)) ||
+        !up(d_order, order.data(), K * sizeof(int)) || cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
+    G.inst = d_inst;
+    G.order = d_order;
+    G.counter = d_counter;
+    G.q_rp = d_qrp;
+    G.a_rp = d_arp;
+    G.at_rp = d_atrp;
+    G.q_ci = d_qci;
+    G.a_ci = d_aci;
+    G.at_ci = d_atci;
+    G.q_v0 = d_qv0;
+    G.a_v0 = d_av0;
+    G.at_v0 = d_atv0;
+    G.c0 = d_c;
+    G.l0 = d_l;
+    G.u0 = d_u;
+    G.AL0 = d_AL;
+    G.AU0 = d_AU;
+    G.nmax = std::max(b->nmax, 1);
+    G.mmax = std::max(b->mmax, 1);
+    *out = b;
+    return HPRQP_STATUS_OK;
+}
+
+HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
+{
+    using namespace hpr;
+    if (!b || !p) return HPRQP_STATUS_INVALID_ARGUMENT;
+    B_CK(cudaSetDevice(b->device));
+    BatchArgs &G = b->args;
+    const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
+    const size_t vec_bytes = (4 * na + 2 * ma) * sizeof(double);
+    G.vec_smem = HPR_BATCH_VEC_SMEM && kScratchBytes + vec_bytes <= kSmemLimit;
+    const size_t smem = kScratchBytes + (G.vec_smem ? vec_bytes : 0);
+    B_CK(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve, kBT, smem));
+    const int grid = std::max(1, std::min((int)b->K, b->num_sms * std::max(per_sm, 1)));
+    // per-CTA workspace (allocated lazily, sized by the grid)
+    const size_t stride = kBatchNVecs * na + kBatchMVecs * ma;
+    if (!G.ws || G.ws_stride != stride) {
+        double *ws = nullptr;
+        HPRQPStatus st = balloc(b, &ws, stride * (size_t)b->num_sms * std::max(per_sm, 1));
+        if (st) return st;
+        G.ws = ws;
+        G.ws_stride = stride;
+    }
+    G.stoptol = p->stoptol;
+    G.max_iter = (long long)std::min<size_t>(p->max_iter, (size_t)LLONG_MAX);
+    G.time_limit = p->time_limit;
+    G.check_iter = (int)p->check_iter;
+    G.print_frequency = p->print_frequency;
+    G.use_scaling = p->use_scaling;
+    unsigned long long *d_t0 = nullptr;
+    HPRQPStatus st = balloc(b, &d_t0, 1);
+    if (st) return st;
+    B_CK(cudaMemsetAsync(G.counter, 0, sizeof(int), b->stream));
+    k_batch_clock<<<1, 1, 0, b->stream>>>(d_t0);
+    count_launch();
+    unsigned long long h_t0 = 0;
+    B_CK(cudaMemcpyAsync(&h_t0, d_t0, sizeof(h_t0), cudaMemcpyDeviceToHost, b->stream));
+    B_CK(cudaStreamSynchronize(b->stream));
+    G.t_start = h_t0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, b->stream);
+    const char *pe = getenv("HPRQP_B200_BATCH_PHASES");
+    unsigned long long *d_phase = nullptr;
+    if (pe && pe[0] == '1') {
+        HPRQPStatus st2 = balloc(b, &d_phase, (size_t)grid * 8);
+        if (st2) return st2;
+        B_CK(cudaMemsetAsync(d_phase, 0, (size_t)grid * 8 * sizeof(unsigned long long), b->stream));
+    }
+    G.phase_clk = d_phase;
+    k_batch_solve<<<grid, kBT, smem, b->stream>>>(G);
+    count_launch();
+    cudaEventRecord(e1, b->stream);
+    cudaError_t err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    B_CK(err);
+    B_CK(cudaGetLastError());
+    b->last_ms = ms;
+    b->solved = true;
+    if (d_phase) {
+        std::vector<unsigned long long> h((size_t)grid * 8);
+        B_CK(cudaMemcpy(h.data(), d_phase, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        double tot[8] = {0};
+        for (int g = 0; g < grid; ++g)
+            for (int q = 0; q < 8; ++q) tot[q] += (double)h[(size_t)g * 8 + q];
+        fprintf(stderr, "[hprqp-b200 batch phases, %% of CTA time] load+scale %.1f setup %.1f power %.1f steps %.1f "
+                        "residuals %.1f m-norm %.1f sigma+restart %.1f (grid %d, smem %zu)\n",
+                100 * tot[0] / tot[7], 100 * tot[1] / tot[7], 100 * tot[2] / tot[7], 100 * tot[3] / tot[7],
+                100 * tot[4] / tot[7], 100 * tot[5] / tot[7], 100 * tot[6] / tot[7], grid, smem);
+    }
+    return HPRQP_STATUS_OK;
+}
+
+double hprqp_batch_last_solve_ms(const HPRQPBatch *b) { return b ? b->last_ms : 0.0; }
+
+size_t hprqp_batch_num_instances(const HPRQPBatch *b) { return b ? b->K : 0; }
+
+HPRQPStatus hprqp_batch_get_results(const HPRQPBatch *b, int *status, size_t *iter, double *primal_obj,
+                                    double *residual, double *gap, double *x, double *y, double *z, double *w)
+{
+    if (!b || !b->solved) return HPRQP_STATUS_INVALID_ARGUMENT;
+    const hpr::BatchArgs &G = b->args;
+    const size_t K = b->K;
+    std::vector<long long> it(K);
+    std::vector<int> stv(K);
+    auto down = [&](void *h, const void *d, size_t bytes) {
+        return cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, b->stream) == cudaSuccess;
+    };
+    if (!down(stv.data(), G.status, K * sizeof(int)) || !down(it.data(), G.iters, K * sizeof(long long)))
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
+    if ((primal_obj && !down(primal_obj, G.pobj, K * 8)) || (residual && !down(residual, G.resid, K * 8)) ||
+        (gap && !down(gap, G.gap, K * 8)))
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
+    std::vector<double> hx, hy;
+    // x, z, w: preprocessing keeps every variable, so the packing matches the caller's
+    if ((x && !down(x, G.x, b->total_n * 8)) || (z && !down(z, G.z, b->total_n * 8)) ||
+        (w && !down(w, G.w, b->total_n * 8)))
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
+    if (y) {
+        hy.resize(std::max<size_t>(b->total_m, 1));
+        if (!down(hy.data(), G.y, b->total_m * 8)) return HPRQP_STATUS_NOT_IMPLEMENTED;
+    }
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return HPRQP_STATUS_NOT_IMPLEMENTED;
+    for (size_t k = 0; k < K; ++k) {
+        if (status) status[k] = stv[k];
+        if (iter) iter[k] = (size_t)it[k];
+    }
+    if (y) {
+        // scatter back to the caller's rows; rows removed by preprocessing get 0
+        std::fill(y, y + b->total_m_orig, 0.0);
+        for (size_t k = 0; k < K; ++k) {
+            const auto &kr = b->kept_rows[k];
+            for (size_t r = 0; r < kr.size(); ++r) y[b->row_off[k] + kr[r]] = hy[b->inst[k].row + r];
+        }
+    }
+    return HPRQP_STATUS_OK;
+}
+
+void hprqp_batch_destroy(HPRQPBatch *b)
+{
+    if (!b) return;
+    hpr::batch_free(b);
+    delete b;
+}
+
+HPRQPStatus hprqp_solve_batch(size_t K, const size_t *var_offsets, const size_t *row_offsets, const HPRQPMatrixCSR *Q,
+                              const HPRQPMatrixCSR *A, const double *c, const double *AL, const double *AU,
+                              const double *l, const double *u, const double *obj_constants,
+                              const HPRQPBatchParams *params, int *status, size_t *iter, double *primal_obj,
+                              double *residual, double *gap, double *x, double *y, double *z, double *w)
+{
+    if (!params) return HPRQP_STATUS_INVALID_ARGUMENT;
+    HPRQPBatch *b = nullptr;
+    HPRQPStatus st = hprqp_batch_create(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants,
+                                        params->device_number, &b);
+    if (st != HPRQP_STATUS_OK) return st;
+    st = hprqp_batch_solve(b, params);
+    if (st == HPRQP_STATUS_OK) st = hprqp_batch_get_results(b, status, iter, primal_obj, residual, gap, x, y, z, w);
+    hprqp_batch_destroy(b);
+    return st;
+}
+
+}  // extern "C"

@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kThreads, HPR_SPMV_MIN_BLOCKS) k_spmv(const DC
 }
 
 // one warp per chunk of a long row: partial sums only
-__global__ void __launch_bounds__(kThreads) k_chunks(const DCsr M, const double *__restrict__ xin)
+static __global__ void __launch_bounds__(kThreads) k_chunks(const DCsr M, const double *__restrict__ xin)
 {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * kWarps + (threadIdx.x >> 5);

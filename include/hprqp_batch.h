@@ -1,0 +1,77 @@
+/*
+ * hprqp_batch.h -- batched solves and the implicit-differentiation adjoint.
+ *
+ * These entry points are additions: the reference (PolyU-IOR/HPR-QP-C) has
+ * no batch API and no adjoint.  Each instance of a batch is solved with the
+ * reference algorithm (same preprocessing, scaling, step, restart and sigma
+ * rules as solve_gpu, reference src/gpu/solver.cu:127-232), to its own
+ * tolerance, with its own sigma and restart state.
+ *
+ * A batch is given as one block-diagonal QP: instance k owns variables
+ * [var_offsets[k], var_offsets[k+1]) and constraint rows
+ * [row_offsets[k], row_offsets[k+1]); Q and A are the block-diagonal
+ * matrices in host CSR form (entries outside an instance's block are
+ * rejected with HPRQP_STATUS_INVALID_ARGUMENT).  All arrays are host memory.
+ */
+#ifndef HPRQP_BATCH_H
+#define HPRQP_BATCH_H
+
+#include <stddef.h>
+
+#include "shared/types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct HPRQPBatch HPRQPBatch;
+
+typedef struct HPRQPBatchParams {
+    double stoptol;      /* per-instance relative KKT tolerance (default 1e-6) */
+    size_t max_iter;     /* per instance (default INT_MAX) */
+    double time_limit;   /* seconds for the whole batch (default 3600) */
+    size_t check_iter;   /* residual / restart cadence (default 100) */
+    int print_frequency; /* -1: adaptive check steps as in HPRQPParams (default) */
+    int use_scaling;     /* Ruiz + Pock-Chambolle (default 1) */
+    int device_number;   /* CUDA device (default 0) */
+    int verbose;         /* unused, reserved */
+} HPRQPBatchParams;
+
+void hprqp_batch_params_set_defaults(HPRQPBatchParams *params);
+
+/* Preprocess every instance (the single-QP builder's rules) and upload the
+ * batch to the device.  The inputs are copied; the handle owns its data. */
+HPRQPStatus hprqp_batch_create(size_t num_instances, const size_t *var_offsets, const size_t *row_offsets,
+                               const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c,
+                               const double *AL, const double *AU, const double *l, const double *u,
+                               const double *obj_constants, int device_number, HPRQPBatch **out);
+
+/* Solve all instances (one persistent kernel; inputs already on the device).
+ * May be called repeatedly; every call starts from the original data. */
+HPRQPStatus hprqp_batch_solve(HPRQPBatch *batch, const HPRQPBatchParams *params);
+
+/* Device time of the last hprqp_batch_solve kernel, milliseconds. */
+double hprqp_batch_last_solve_ms(const HPRQPBatch *batch);
+size_t hprqp_batch_num_instances(const HPRQPBatch *batch);
+
+/* Copy results to host arrays (any pointer may be NULL).  Per instance:
+ * status (HPRQPStatus), iter, primal objective, KKT residual, relative gap.
+ * Packed like the inputs: x, z, w (total variables) and y (total rows; rows
+ * removed by preprocessing -- empty or free on both sides -- get 0). */
+HPRQPStatus hprqp_batch_get_results(const HPRQPBatch *batch, int *status, size_t *iter, double *primal_obj,
+                                    double *residual, double *gap, double *x, double *y, double *z, double *w);
+
+void hprqp_batch_destroy(HPRQPBatch *batch);
+
+/* One-call form: create + solve + get_results + destroy. */
+HPRQPStatus hprqp_solve_batch(size_t num_instances, const size_t *var_offsets, const size_t *row_offsets,
+                              const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c, const double *AL,
+                              const double *AU, const double *l, const double *u, const double *obj_constants,
+                              const HPRQPBatchParams *params, int *status, size_t *iter, double *primal_obj,
+                              double *residual, double *gap, double *x, double *y, double *z, double *w);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

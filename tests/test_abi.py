@@ -115,3 +115,16 @@ def test_no_host_stub_exits(engine_lib):
                          text=True).stdout
     names = {line.split()[-1].split("@")[0] for line in out.splitlines() if line.strip()}
     assert "exit" not in names and "_exit" not in names
+
+
+def test_batch_rejects_bad_packing(engine_lib):
+    """hprqp_batch_create validates the block-diagonal packing on the host."""
+    import hprqp
+    from hprqp import batch
+
+    insts = instances.tiny_cases()[:2]
+    p = batch.pack(insts)
+    p.var_offsets = p.var_offsets.copy()
+    p.var_offsets[-1] += 1  # does not end at n
+    with pytest.raises(RuntimeError, match="INVALID_ARGUMENT"):
+        batch.Batch(p)

@@ -1,0 +1,118 @@
+"""Batched persistent solver vs the CPU oracle and the plain path.
+
+Each instance of a batch must behave like a single solve of the same QP:
+same status, objective within 1e-6 relative of the oracle, iterates after K
+steps within 1e-8 (the plain-path tolerance), host-recomputed KKT within the
+requested tolerance."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import pyoracle
+from hprqp import instances
+
+pytestmark = pytest.mark.gpu
+
+
+def _kept(inst):
+    """rows that survive preprocessing (non-empty, not free on both sides)"""
+    lens = np.diff(np.asarray(inst.A.indptr))
+    free = np.isneginf(inst.AL) & np.isposinf(inst.AU)
+    return np.nonzero((lens > 0) & ~free)[0]
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    if a.size == 0:
+        return 0.0
+    return float(np.max(np.abs(a - b)) / max(1.0, float(np.max(np.abs(b)))))
+
+
+TINY = [i for i in instances.tiny_cases() if i.name != "tall_diag"]
+
+
+@pytest.mark.parametrize("cap", [1, 10, 100, 250])
+def test_batch_iterates_after_k_steps(engine_lib, cap):
+    from hprqp import batch
+
+    insts = instances.tiny_cases()
+    b = batch.Batch(insts)
+    b.solve(stoptol=1e-8, max_iter=cap)
+    r = b.results()
+    xs, ys, zs, ws = b.split(r.x, "x"), b.split(r.y, "y"), b.split(r.z, "x"), b.split(r.w, "x")
+    for k, inst in enumerate(insts):
+        om = pyoracle.OracleModel(inst)
+        o = om.solve(stoptol=1e-8, max_iter=cap, mode=pyoracle.MODE_GPU_REF)
+        assert r.status[k] == o["status"], inst.name
+        assert r.iter[k] == o["iter"], inst.name
+        # rows removed by preprocessing come back as 0; the oracle reports the kept rows
+        kept_y = ys[k][_kept(inst)]
+        for got, ref in ((xs[k], o["x"]), (kept_y, o["y"]), (zs[k], o["z"]), (ws[k], o["w"])):
+            assert _rel(got, ref) <= 1e-8, inst.name
+
+
+def test_batch_tiny_converge(engine_lib):
+    from hprqp import batch
+
+    r = batch.solve_batch(TINY, stoptol=1e-8)
+    for k, inst in enumerate(TINY):
+        o = pyoracle.OracleModel(inst).solve(stoptol=1e-8, mode=pyoracle.MODE_GPU_REF)
+        assert r.status[k] == 6 == o["status"], inst.name
+        assert abs(r.objective[k] - o["primal_obj"]) <= 1e-6 * max(1.0, abs(o["primal_obj"]))
+
+
+def test_batch_seeded_matches_oracle_and_plain(engine_lib):
+    """Instances of the 4096-QP recipe: batch == plain solve == oracle."""
+    hprqp = engine_lib
+    from hprqp import batch
+
+    insts = [instances.config3_instance(k) for k in range(12)]
+    b = batch.Batch(insts)
+    ms = b.solve(stoptol=1e-6)
+    assert ms > 0
+    r = b.results()
+    xs, ys, zs = b.split(r.x, "x"), b.split(r.y, "y"), b.split(r.z, "x")
+    for k, inst in enumerate(insts):
+        om = pyoracle.OracleModel(inst)
+        o = om.solve(stoptol=1e-6, mode=pyoracle.MODE_GPU_REF)
+        assert r.status[k] == 6 == o["status"], k
+        assert abs(r.objective[k] - o["primal_obj"]) <= 1e-6 * abs(o["primal_obj"]), k
+        assert abs(int(r.iter[k]) - o["iter"]) <= max(20, o["iter"] // 10), (k, r.iter[k], o["iter"])
+        kkt = om.kkt(xs[k], ys[k][_kept(inst)], zs[k])["kkt"]
+        assert kkt <= 1.01e-6, (k, kkt)
+        p = hprqp.optimize(hprqp.build_from_instance(inst), hprqp.Parameters(verbose=False, stoptol=1e-6))
+        assert abs(p.objective - r.objective[k]) <= 1e-6 * abs(p.objective)
+
+
+def test_batch_resolve_is_deterministic(engine_lib):
+    from hprqp import batch
+
+    insts = [instances.config3_instance(k) for k in range(20, 28)]
+    b = batch.Batch(insts)
+    b.solve(stoptol=1e-6)
+    r1 = b.results()
+    b.solve(stoptol=1e-6)
+    r2 = b.results()
+    assert np.array_equal(r1.iter, r2.iter)
+    assert np.array_equal(r1.x, r2.x) and np.array_equal(r1.y, r2.y)
+
+
+def test_batch_noc_and_empty_rows(engine_lib):
+    """free variables (noC path) and rows removed by preprocessing."""
+    from hprqp import batch
+
+    free = instances.plain_qp(0x48505251 + 90100, n=50, m=20, a_density=0.1, m_rows=10, m_density=0.1, n_eq=12)
+    free.l[:] = -np.inf
+    free.u[:] = np.inf
+    holes = instances.plain_qp(0x48505251 + 90200, n=40, m=16, a_density=0.1, m_rows=8, m_density=0.1, n_eq=8)
+    holes.AL[3] = -np.inf
+    holes.AU[3] = np.inf  # a free row: deleted by preprocessing
+    insts = [free, holes]
+    r = batch.solve_batch(insts, stoptol=1e-6)
+    for k, inst in enumerate(insts):
+        o = pyoracle.OracleModel(inst).solve(stoptol=1e-6, mode=pyoracle.MODE_GPU_REF)
+        assert r.status[k] == 6 == o["status"]
+        assert abs(r.objective[k] - o["primal_obj"]) <= 1e-6 * max(1.0, abs(o["primal_obj"]))
+    ys = np.split(r.y, np.cumsum([i.m for i in insts])[:-1])
+    assert ys[1][3] == 0.0 and len(ys[1]) == holes.m
