@@ -40,6 +40,29 @@ HPRQPStatus hprqp_b200_setup(const HPRQPModel *model, const HPRQPParams *params,
                              double *row_norm, double *col_norm, double *q_val, double *a_val,
                              double *at_val, double *c, double *l, double *u, double *AL, double *AU);
 
+/* lambda_max(A A') * 1.05 -- the dual step-size bound that solve_gpu computes
+ * at setup -- by the same power iteration, for callers that cannot allocate
+ * device memory (their GPU memory belongs to another allocator or arena, or
+ * device allocation is not allowed while they run).  No counterpart in the
+ * reference, which only computes this inside its own setup.
+ *
+ * Inputs are device arrays owned by the caller: A (m x n) and its transpose
+ * A' (n x m) in 0-based int32 CSR (row pointers, column indices, values),
+ * which must be valid CSR of those shapes.  The result and the iteration
+ * count are written to host memory.  `stream` is a cudaStream_t (NULL for the
+ * legacy default stream); the call returns after the stream has executed it.
+ * All work vectors live in one fixed 8 MiB device array inside this library:
+ * 2*m + n must not exceed 1,046,526 (larger calls return
+ * HPRQP_STATUS_INVALID_ARGUMENT).  The array is shared by all calls and
+ * keeps the previous call's contents, so calls on the same device must not
+ * overlap in time.  The first call on a device looks up the array's device
+ * address; make it before any stream capture on that device.  Nothing is
+ * allocated: no cudaMalloc, no cudaFree, no allocating library call. */
+HPRQPStatus hprqp_b200_power_lambda_noalloc(int device, size_t m, size_t n, const int *a_row_ptr,
+                                            const int *a_col, const double *a_val, const int *at_row_ptr,
+                                            const int *at_col, const double *at_val, void *stream,
+                                            double *lambda_out, int *iterations_out);
+
 /* Number of engine kernel launches issued by this process so far
  * (graph replays count each captured kernel). */
 uint64_t hprqp_b200_launch_count(void);
