@@ -1,29 +1,31 @@
 """Benchmark of the HPR-QP engine on one node.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload batch|plain]
 
-Metric (the project's headline): solves/s to 1e-6 relative KKT on the
-4096-instance batch workload (n ~ U{50..2000}, m ~ U{n/4..n}, seeded), next
-to the plain one-QP-per-call path, plus the SpMV bandwidth of the large
-power-law QP (n=1e6, m=5e5, nnz(A)~1e7, nnz(Q)~3.2e7) against the measured
-HBM peak.
+Metric: solves/s to 1e-6 relative KKT on the 4096-QP batch workload
+(n ~ U{50..2000}, m ~ U{ceil(n/4)..n}, A density U(0.5%,5%), Q = M'M + 0.01 I
+with nnz(Q) ~ dQ n^2, dQ ~ U(0.1%,2%), 60% equality rows, seeded), next to
+looping the plain one-QP-per-call solve over the same instances, plus the
+SpMV bandwidth on the large power-law QP (n=1e6, m=5e5, nnz(A)~1e7,
+nnz(Q)~3.2e7) against the measured HBM peak.
 
-One step = one pass of the solver over the whole batch of synthetic QPs.
-``value`` is measured with the inputs already resident on the device;
-``e2e`` goes through the C ABI with host buffers (host->device copies and the
-read-back of the solutions inside the timed region).  Multi-GPU runs are
-replicas: every rank solves its own copy of the batch (weak scaling), and the
-time is the max over ranks.
+One step = one batched solve of the whole 4096-instance batch.  ``value`` is
+measured with the batch resident on the device (CUDA-event time of the solve
+kernel); ``e2e`` goes through the one-call C ABI (hprqp_solve_batch) from
+host buffers, so host preprocessing, upload and read-back of all solutions
+are inside the timed region.  Multi-GPU runs are replicas: every rank solves
+its own batch (different seeds), the time is the max over ranks.
 
-``--impl reference`` times the reference's own CPU implementation of the path
-(oracle/_ref/libhprqp_ref_cpu.so, compiled from the reference sources; the
-C oracle when that library is absent) on the host cores, on a bounded sample
-of the same workload.
+``--impl reference`` times the reference's own CPU implementation
+(oracle/_ref/libhprqp_ref_cpu.so, compiled from the reference sources; the C
+oracle port if that library is absent) on the host cores, one process per
+core, on a bounded sample of the same instances per step.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
+import datetime
 import json
 import multiprocessing as mp
 import os
@@ -41,6 +43,7 @@ sys.path.insert(0, str(ROOT / "oracle"))
 
 METRIC = "solves/s to 1e-6 rel-KKT, batched vs plain on 1 B200; SpMV GB/s vs HBM peak"
 STOPTOL = 1e-6
+BATCH = 4096
 
 
 def _peaks():
@@ -51,10 +54,9 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-# --------------------------------------------------------------------------
-# clocks sampling during the timed region
-# --------------------------------------------------------------------------
 class ClockSampler:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -82,18 +84,24 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.path.exists():
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = []
-        for line in self.path.read_text().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        self.path.unlink(missing_ok=True)
+        if self.path.exists():
+            for line in self.path.read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            self.path.unlink(missing_ok=True)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
@@ -101,7 +109,7 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------
-# workloads
+# workload
 # --------------------------------------------------------------------------
 def batch_instances(count: int, start: int = 0):
     from hprqp import instances
@@ -109,7 +117,7 @@ def batch_instances(count: int, start: int = 0):
     return instances.config3(count, start)
 
 
-def algorithmic_bytes_per_iter(inst) -> float:
+def bytes_per_iter(inst) -> float:
     """B_iter = 2 S(Q) + S(A) + S(A') + 8 (24 n + 7 m), S(M) = 12 nnz + 4 (nrow+1)."""
     n, m = inst.n, inst.m
     sq = 12 * inst.Q.nnz + 4 * (n + 1)
@@ -122,35 +130,35 @@ def _ref_worker(args):
     inst_ids, stoptol = args
     import pyoracle
 
-    out = []
+    statuses = []
     for k in inst_ids:
         inst = batch_instances(1, k)[0]
         if pyoracle.ref_available():
             r = pyoracle.ref_solve(inst, stoptol=stoptol)
         else:
             r = pyoracle.OracleModel(inst).solve(stoptol=stoptol, mode=pyoracle.MODE_CPU_REF)
-        out.append(int(r["status"]))
-    return out
+        statuses.append(int(r["status"]))
+    return statuses
 
 
-def cpu_reference_rate(sample: int, cores: int):
-    """Reference CPU solves/s over `sample` batch instances on `cores` host
-    processes (spawned, one instance at a time per process)."""
+def cpu_reference_rate(ids, cores: int):
+    """Reference CPU solves/s over the given batch instances on `cores`
+    spawned processes."""
     import pyoracle
 
     kind = "reference" if pyoracle.ref_available() else "port"
-    ids = list(range(sample))
     chunks = [ids[i::cores] for i in range(cores)]
     ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
+        pool.map(int, range(cores))  # start the workers outside the timed region
+        t0 = time.perf_counter()
         statuses = sum(pool.map(_ref_worker, [(c, STOPTOL) for c in chunks if c]), [])
-    dt = time.perf_counter() - t0
-    return sample / dt, kind, dt, statuses
+        dt = time.perf_counter() - t0
+    return len(ids) / dt, kind, dt, statuses
 
 
-def spmv_roofline(peak_gbs: float):
-    """Row-block SpMV on the large power-law QP's A, A' and Q."""
+def spmv_leg(peak_gbs: float, reps: int = 10):
+    """Row-tiled SpMV on the large power-law QP's A and Q (device timing)."""
     import hprqp
     from hprqp import instances
 
@@ -162,26 +170,59 @@ def spmv_roofline(peak_gbs: float):
         "Q": (inst.Q.indptr, inst.Q.indices, inst.Q.data, inst.n, inst.n),
     }.items():
         x = rng.standard_normal(ncol)
-        _, ms = hprqp.spmv(ip, ii, dd, ncol, x, reps=10)
+        _, ms = hprqp.spmv(ip, ii, dd, ncol, x, reps=reps)
         nnz = int(ip[-1])
         algo = 12 * nnz + 4 * (nrow + 1) + 8 * ncol + 8 * nrow
         gbs = algo / (ms * 1e-3) / 1e9
-        out[name] = {"nnz": nnz, "ms": ms, "GB/s": gbs, "frac": gbs / peak_gbs, "bytes": algo}
+        out[name] = {"nnz": nnz, "ms": round(ms, 4), "GB/s": round(gbs, 1), "frac": round(gbs / peak_gbs, 4),
+                     "bytes": algo}
     return out
 
 
-def run_plain(instances_list, params_kw):
+def e2e_step(packed, device: int):
+    """One call of hprqp_solve_batch from host buffers; returns seconds."""
+    from hprqp import batch as hb
     import hprqp
 
-    models = [hprqp.build_from_instance(inst) for inst in instances_list]
-    params = hprqp.Parameters(verbose=False, stoptol=STOPTOL, **params_kw)
-    iters = []
-    ok = 0
-    for mdl in models:
-        r = hprqp.optimize(mdl, params, as_numpy=True)
-        iters.append(r.iter)
-        ok += r.status_code == hprqp.STATUS_OPTIMAL
-    return iters, ok
+    lib = hprqp._lib()
+    hb._configure()
+    fn = lib.hprqp_solve_batch
+    c_size_p = ctypes.POINTER(ctypes.c_size_t)
+    c_double_p = ctypes.POINTER(ctypes.c_double)
+    fn.argtypes = [ctypes.c_size_t, c_size_p, c_size_p, ctypes.POINTER(hprqp._MatrixCSR),
+                   ctypes.POINTER(hprqp._MatrixCSR), c_double_p, c_double_p, c_double_p, c_double_p, c_double_p,
+                   c_double_p, ctypes.POINTER(hb.BatchParams), ctypes.POINTER(ctypes.c_int), c_size_p, c_double_p,
+                   c_double_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p]
+    p = packed
+    K = p.K
+    n = int(p.var_offsets[-1])
+    m = int(p.row_offsets[-1])
+    keep = []
+    Q = hb._csr(n, n, p.q_indptr, p.q_indices, p.q_data, keep)
+    A = hb._csr(m, n, p.a_indptr, p.a_indices, p.a_data, keep)
+    dp = lambda a: a.ctypes.data_as(c_double_p)  # noqa: E731
+    status = np.zeros(K, np.int32)
+    it = np.zeros(K, np.uint64)
+    obj = np.zeros(K)
+    res = np.zeros(K)
+    gap = np.zeros(K)
+    x = np.zeros(n)
+    y = np.zeros(max(m, 1))
+    z = np.zeros(n)
+    w = np.zeros(n)
+    params = hb.default_params(stoptol=STOPTOL, device_number=device)
+    vo = np.ascontiguousarray(p.var_offsets, np.uint64)
+    ro = np.ascontiguousarray(p.row_offsets, np.uint64)
+    t0 = time.perf_counter()
+    st = fn(K, vo.ctypes.data_as(c_size_p), ro.ctypes.data_as(c_size_p), ctypes.byref(Q), ctypes.byref(A), dp(p.c),
+            dp(p.AL), dp(p.AU), dp(p.l), dp(p.u), dp(p.obj), ctypes.byref(params),
+            status.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), it.ctypes.data_as(c_size_p), dp(obj), dp(res),
+            dp(gap), dp(x), dp(y), dp(z), dp(w))
+    dt = time.perf_counter() - t0
+    if st != 0:
+        raise RuntimeError(f"hprqp_solve_batch failed: {st}")
+    d2h = status.nbytes + it.nbytes + obj.nbytes + res.nbytes + gap.nbytes + x.nbytes + 8 * m + z.nbytes + w.nbytes
+    return dt, int(np.sum(status == 6)), d2h
 
 
 # --------------------------------------------------------------------------
@@ -193,110 +234,151 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain", choices=["plain"])
-    ap.add_argument("--batch", type=int, default=64, help="instances per step")
-    ap.add_argument("--cpu-sample", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=BATCH, help="instances per step")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--no-spmv", action="store_true")
+    ap.add_argument("--only", choices=["spmv", "batch"], default=None,
+                    help="profiling sub-runs: only the large-QP SpMV leg, or only the batched solve")
+    ap.add_argument("--spmv-reps", type=int, default=10)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     cores = os.cpu_count() or 1
-
-    config = {"workload": f"config3 batch: {args.batch} seeded QPs, n~U{{50..2000}}, m~U{{n/4..n}}, "
-                          f"stoptol {STOPTOL:g}",
-              "global_batch": args.batch * world, "parallelism": f"replicas x{world}",
-              "l2": "inputs larger than L2 (126 MB) across a step"}
+    config = {"workload": f"batch of {args.batch} seeded QPs per GPU: n~U{{50..2000}}, m~U{{ceil(n/4)..n}}, "
+                          f"A density U(0.5%,5%), nnz(Q)~U(0.1%,2%) n^2, 60% equality rows; stoptol {STOPTOL:g}",
+              "global_batch": args.batch * world, "parallelism": f"replicas x{world} (instance-sharded)",
+              "l2": "inputs larger than L2: the batch holds ~3 GB of matrices"}
 
     if args.impl == "reference":
         if rank != 0:
             return
+        sample = min(args.cpu_sample, args.batch)
         rates = []
-        kind = "port"
-        for _ in range(args.warmup):
-            pass  # the CPU reference has no warm-up state; warm-up steps are skipped
         t_total = 0.0
-        for _ in range(args.steps):
-            rate, kind, dt, _ = cpu_reference_rate(args.cpu_sample, cores)
+        kind = "port"
+        for step in range(args.steps):
+            ids = list(range(step * sample, (step + 1) * sample))
+            rate, kind, dt, _ = cpu_reference_rate(ids, cores)
             rates.append(rate)
             t_total += dt
         value = float(statistics.median(rates))
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators)",
                 "config": config, "impl": "reference",
                 "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": kind,
-                                 "sample": f"{args.cpu_sample} batch instances per step"},
+                                 "sample": f"{sample} batch instances per step, one process per core"},
                 "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        print(json.dumps(line), flush=True)
         return
 
     import torch
 
     torch.cuda.set_device(local_rank)
+    dist = None
     if world > 1:
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=900))
     import hprqp
+    from hprqp import batch as hb
 
     peak, peak_kind = _peaks()
-    insts = batch_instances(args.batch, 1000 * rank)
-    params_kw = {"device_number": local_rank}
-    for _ in range(args.warmup):
-        run_plain(insts, params_kw)
+    if args.only == "spmv":
+        print(json.dumps({"spmv": spmv_leg(peak, args.spmv_reps)}), flush=True)
+        return
+    insts = batch_instances(args.batch, 100000 * rank)
+    packed = hb.pack(insts)
+    bytes_algo_per_inst = np.array([bytes_per_iter(i) for i in insts])
+    b = hb.Batch(packed, device_number=local_rank)
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
+        if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        b.solve(stoptol=STOPTOL)
     launches0 = hprqp.launch_count()
+    kernel_ms = []
     with ClockSampler(local_rank) as clk:
         barrier()
         t0 = time.perf_counter()
-        iters_all = []
         for _ in range(args.steps):
-            iters, ok = run_plain(insts, params_kw)
-            iters_all.extend(iters)
+            kernel_ms.append(b.solve(stoptol=STOPTOL))
         barrier()
-        dt = time.perf_counter() - t0
+        wall = time.perf_counter() - t0
     launches = hprqp.launch_count() - launches0
-    if world > 1:
-        import torch.distributed as dist
+    res = b.results(vectors=False)
+    dev_s = max_over_ranks(sum(kernel_ms) / 1e3)
+    wall = max_over_ranks(wall)
+    value = args.batch * world * args.steps / dev_s
+    iters = res.iter.astype(np.float64)
+    algo_bytes = float(np.sum(iters * bytes_algo_per_inst))
+    achieved = algo_bytes / (statistics.mean(kernel_ms) / 1e3) / 1e9
+    b.close()
+    if args.only == "batch":
+        print(json.dumps({"value": value, "unit": "solves/s", "kernel_ms": kernel_ms, "achieved_GBs": achieved,
+                          "algorithmic_bytes_per_launch": algo_bytes, "mean_iters": float(iters.mean())}), flush=True)
+        return
 
-        t = torch.tensor([dt], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dt = float(t.item())
-    value = args.batch * world * args.steps / dt
+    # end to end through the C ABI from host buffers
+    e2e_times = []
+    d2h = 0
+    e2e_ok = 0
+    barrier()
+    for _ in range(args.e2e_steps):
+        dt, ok, d2h = e2e_step(packed, local_rank)
+        e2e_times.append(dt)
+        e2e_ok = ok
+    e2e_s = max_over_ranks(sum(e2e_times))
+    e2e_value = args.batch * world * args.e2e_steps / e2e_s
+    h2d = int(packed.q_indptr.size * 4 + packed.q_indices.size * 4 + packed.q_data.nbytes +
+              2 * (packed.a_indices.size * 4 + packed.a_data.nbytes) + 4 * (packed.a_indptr.size + packed.q_indptr.size)
+              + packed.c.nbytes + packed.l.nbytes + packed.u.nbytes + packed.AL.nbytes + packed.AU.nbytes)
 
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators)",
             "config": config, "clocks": clk.summary(), "gpu_launches": int(launches),
-            "e2e": {"value": value, "unit": "solves/s",
-                    "h2d_bytes_per_step": int(sum(12 * i.Q.nnz + 12 * i.A.nnz + 8 * (3 * i.n + 2 * i.m)
-                                                  for i in insts)),
-                    "d2h_bytes_per_step": int(sum(8 * (3 * i.n + i.m) for i in insts))},
-            "mean_iters": float(np.mean(iters_all))}
-    if rank == 0 and not args.no_spmv:
-        sp = spmv_roofline(peak)
-        line["roofline"] = {"bound": "hbm", "achieved": sp["Q"]["GB/s"], "peak": peak, "unit": "GB/s",
-                            "frac": sp["Q"]["GB/s"] / peak, "traffic": None,
-                            "kernel": "k_rowblock<EpiStore> (y = Q x, n=1e6, nnz 3.2e7)",
-                            "peak_kind": peak_kind}
-        line["spmv"] = sp
-    if rank == 0:
-        rate, kind, cdt, _ = cpu_reference_rate(min(args.cpu_sample, 32), cores)
-        line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind,
-                                "sample": f"{min(args.cpu_sample, 32)} batch instances"}
-        print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h),
+                    "optimal": e2e_ok},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_batch_solve",
+                         "algorithmic_bytes_per_launch": algo_bytes, "peak_kind": peak_kind},
+            "solved_optimal": int(np.sum(res.status == 6)), "mean_iters": float(iters.mean())}
 
+    if rank == 0:
+        # plain path: one solve_gpu call per QP over a sample of the same batch
+        sample = insts[:args.plain_sample]
+        models = [hprqp.build_from_instance(i) for i in sample]
+        params = hprqp.Parameters(verbose=False, stoptol=STOPTOL, device_number=local_rank)
+        hprqp.optimize(models[0], params)
+        t0 = time.perf_counter()
+        for mdl in models:
+            hprqp.optimize(mdl, params)
+        plain_rate = len(models) / (time.perf_counter() - t0)
+        line["plain"] = {"value": plain_rate, "unit": "solves/s", "sample": f"{len(models)} instances of the batch"}
+        line["batched_over_plain"] = value / world / plain_rate
+        if not args.no_spmv:
+            line["spmv"] = spmv_leg(peak)
+        ids = list(range(min(args.cpu_sample, args.batch)))
+        rate, kind, cdt, _ = cpu_reference_rate(ids, cores)
+        line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind,
+                                "sample": f"{len(ids)} batch instances, one process per core"}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
         dist.destroy_process_group()
 
 
