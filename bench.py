@@ -179,6 +179,39 @@ def spmv_leg(peak_gbs: float, reps: int = 10):
     return out
 
 
+def adjoint_leg(device: int, count: int = 256, reps: int = 3):
+    """Differentiation workload: 256 QPs (n=500, m=300, 150 equality rows),
+    forward solve to 1e-8, loss L = sum g.x* with g ~ N(0,1) per instance,
+    backward through the device adjoint (MINRES on the active-set KKT
+    system).  Device times of the solve kernel and of the adjoint kernel,
+    plus host wall time of the whole backward call (adjoint + gradient
+    assembly for c, l, u, AL, AU and the nonzeros of Q and A)."""
+    from hprqp import batch as hb
+    from hprqp import instances
+
+    insts = instances.config4(count)
+    b = hb.Batch(insts, device_number=device)
+    rng = np.random.default_rng(4)
+    gx = rng.standard_normal(b.n)
+    fwd, bwd, bwd_wall = [], [], []
+    for _ in range(reps + 1):
+        fwd.append(b.solve(stoptol=1e-8))
+        t0 = time.perf_counter()
+        g = b.backward(gx)
+        bwd_wall.append(1e3 * (time.perf_counter() - t0))
+        bwd.append(g.backward_ms)
+    res = b.results(vectors=False)
+    b.close()
+    f = statistics.median(fwd[1:])
+    k = statistics.median(bwd[1:])
+    w = statistics.median(bwd_wall[1:])
+    return {"workload": f"{count} QPs n=500 m=300 (150 equality), stoptol 1e-8, L = sum g.x*",
+            "forward_kernel_ms": round(f, 3), "backward_kernel_ms": round(k, 3), "backward_call_ms": round(w, 3),
+            "backward_over_forward": round(w / f, 4), "backward_kernel_over_forward": round(k / f, 4),
+            "optimal": int(np.sum(res.status == 6)), "mean_solve_iters": float(res.iter.mean()),
+            "mean_minres_iters": float(g.minres_iters.mean()), "max_minres_relres": float(g.minres_relres.max())}
+
+
 def e2e_step(packed, device: int):
     """One call of hprqp_solve_batch from host buffers; returns seconds."""
     from hprqp import batch as hb
@@ -239,8 +272,9 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--no-spmv", action="store_true")
-    ap.add_argument("--only", choices=["spmv", "batch"], default=None,
-                    help="profiling sub-runs: only the large-QP SpMV leg, or only the batched solve")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--only", choices=["spmv", "batch", "adjoint"], default=None,
+                    help="profiling sub-runs: only the large-QP SpMV leg, the batched solve, or the adjoint")
     ap.add_argument("--spmv-reps", type=int, default=10)
     args = ap.parse_args()
 
@@ -290,6 +324,9 @@ def main():
     peak, peak_kind = _peaks()
     if args.only == "spmv":
         print(json.dumps({"spmv": spmv_leg(peak, args.spmv_reps)}), flush=True)
+        return
+    if args.only == "adjoint":
+        print(json.dumps({"adjoint": adjoint_leg(local_rank)}), flush=True)
         return
     insts = batch_instances(args.batch, 100000 * rank)
     packed = hb.pack(insts)
@@ -373,6 +410,8 @@ def main():
         line["batched_over_plain"] = value / world / plain_rate
         if not args.no_spmv:
             line["spmv"] = spmv_leg(peak)
+        if not args.no_adjoint:
+            line["adjoint"] = adjoint_leg(local_rank)
         ids = list(range(min(args.cpu_sample, args.batch)))
         rate, kind, cdt, _ = cpu_reference_rate(ids, cores)
         line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind,

@@ -86,6 +86,7 @@ struct BatchArgs {
     unsigned long long *phase_clk;  // optional [grid x 8] clock64 totals per phase
     unsigned char *active_x;  // 1 = variable at a bound (for the adjoint)
     unsigned char *active_r;  // 1 = row at a bound
+    double *col_norm_out, *row_norm_out;  // scaling of each instance (for the adjoint)
 };
 
 // optional per-CTA phase clocks: 0 load+scale, 1 setup norms/diag, 2 power
@@ -971,10 +972,12 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             B.w[I.var + i] = V.w_bar[i] / cn;
             B.z[I.var + i] = V.z_bar[i] * cn;
             if (B.active_x) B.active_x[I.var + i] = V.z_bar[i] != 0.0;
+            B.col_norm_out[I.var + i] = cn;
         }
         for (int i = tid; i < m; i += kBT) {
             B.y[I.row + i] = V.y_bar[i] / V.row_norm[i];
             if (B.active_r) B.active_r[I.row + i] = V.y_bar[i] != 0.0;
+            B.row_norm_out[I.row + i] = V.row_norm[i];
         }
         if (B.phase_clk && tid == 0) B.phase_clk[blockIdx.x * 8 + 7] += (unsigned long long)(clock64() - _ptot);
         if (tid == 0) {
@@ -984,6 +987,193 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             B.resid[k] = S.kkt;
             B.gap[k] = S.gap;
             B.restarts[k] = (int)S.times;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// implicit-differentiation adjoint: MINRES on the active-set KKT operator
+// ---------------------------------------------------------------------------
+// For each instance, with F = {i : z_i == 0} (variables off their bounds)
+// and R = {r : y_r != 0} (rows at a bound), solve
+//     [[Q_FF, A_RF'], [A_RF, 0]] [lam_F; mu_R] = [gx_F; -gy_R]
+// matrix-free.  The solve runs on the scaled matrices the last
+// hprqp_batch_solve left on the device: with D = diag(col_norm, row_norm),
+// K = D Ks D, so Ks (D lam) = D^-1 rhs and lam = D^-1 sol.  The operator is
+// applied as P Ks P with P the 0/1 active-set mask (read from z and y), so
+// every Krylov vector stays inside the active subspace.  MINRES is the
+// Paige-Saunders recurrence (Lanczos three-term step + Givens QR of the
+// tridiagonal), one instance per CTA; the three Lanczos vectors, which are
+// the SpMV gather sources, live in shared memory when they fit.
+struct AdjArgs {
+    int K;
+    const BInst *inst;
+    const int *order;
+    int *counter;
+    const int *q_rp, *q_ci, *a_rp, *a_ci, *at_rp, *at_ci;
+    const double *q_v, *a_v, *at_v;             // scaled matrices left by the last solve
+    const double *col_norm, *row_norm, *z, *y;  // per instance, packed
+    const double *gx, *gy;                      // loss gradients (packed; gy may be null)
+    double *lam_x, *lam_y;                      // outputs: lambda, mu (original space)
+    int *iters;
+    double *relres;
+    double tol;
+    int maxit_factor;
+    double *ws;
+    size_t ws_stride;
+    int nmax, mmax;
+    int lanczos_smem;  // 1: the Lanczos vectors live in shared memory
+};
+
+constexpr int kAdjGlobalN = 5, kAdjGlobalM = 4;  // sol, w_old, w, w_new (+ Q v) per CTA in global memory
+constexpr int kAdjLanczos = 3;                   // v_old, v, v_new (n and m parts)
+
+__global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_adjoint(const AdjArgs B)
+{
+    extern __shared__ __align__(16) double dyn_smem[];
+    double *scratch = dyn_smem;
+    __shared__ double s_red[kBW][8];
+    __shared__ double s_out[8];
+    __shared__ int s_inst;
+    const int tid = threadIdx.x;
+    const int na = (B.nmax + 31) & ~31, ma = (B.mmax + 31) & ~31;
+    double *g = B.ws + (size_t)blockIdx.x * B.ws_stride;
+    double *lz = B.lanczos_smem ? dyn_smem + kBW * kWin
+                                : g + kAdjGlobalN * (size_t)na + kAdjGlobalM * (size_t)ma;
+    for (;;) {
+        if (tid == 0) {
+            const int slot = atomicAdd(B.counter, 1);
+            s_inst = slot < B.K ? B.order[slot] : -1;
+        }
+        __syncthreads();
+        const int k = s_inst;
+        __syncthreads();
+        if (k < 0) break;
+        const BInst I = B.inst[k];
+        const int n = I.n, m = I.m;
+        const LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz};
+        const LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz};
+        const LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz};
+        const double *cn = B.col_norm + I.var, *rn = B.row_norm + I.row;
+        const double *zk = B.z + I.var, *yk = B.y + I.row;
+        double *sol_n = g, *wo_n = g + na, *w_n = g + 2 * na, *wn_n = g + 3 * na, *tmp = g + 4 * na;
+        double *gm = g + kAdjGlobalN * (size_t)na;
+        double *sol_m = gm, *wo_m = gm + ma, *w_m = gm + 2 * ma, *wn_m = gm + 3 * ma;
+        double *vo_n = lz, *v_n = lz + na, *vn_n = lz + 2 * na;
+        double *vo_m = lz + 3 * na, *v_m = lz + 3 * na + ma, *vn_m = lz + 3 * na + 2 * ma;
+        const int ops1[1] = {kSum};
+        double b2[1] = {0.0};
+        for (int i = tid; i < n; i += kBT) {
+            const double rhs = zk[i] == 0.0 ? B.gx[I.var + i] / cn[i] : 0.0;  // D^-1 P rhs
+            v_n[i] = rhs;
+            b2[0] += rhs * rhs;
+            sol_n[i] = vo_n[i] = wo_n[i] = w_n[i] = 0.0;
+        }
+        for (int r = tid; r < m; r += kBT) {
+            const double rhs = (B.gy && yk[r] != 0.0) ? -B.gy[I.row + r] / rn[r] : 0.0;
+            v_m[r] = rhs;
+            b2[0] += rhs * rhs;
+            sol_m[r] = vo_m[r] = wo_m[r] = w_m[r] = 0.0;
+        }
+        cta_allreduce<1>(b2, ops1, s_red, s_out);
+        const double beta0 = sqrt(b2[0]);
+        double beta = beta0, eta = beta0;
+        double c_old = 1.0, c = 1.0, s_old = 0.0, s = 0.0;
+        int it = 0;
+        if (beta0 > 0.0) {
+            const double inv = 1.0 / beta0;
+            for (int i = tid; i < n; i += kBT) v_n[i] *= inv;
+            for (int r = tid; r < m; r += kBT) v_m[r] *= inv;
+            __syncthreads();
+            const int maxit = B.maxit_factor * (n + m) + 100;
+            for (it = 0; it < maxit; ++it) {
+                // v_new = P Ks P v.  Q and A' have the same 32-row tiling, so
+                // tmp[i] is written and read by the same thread.
+                if (m > 0) {
+                    cta_spmv(Q, v_n, scratch, [&](int i, double q) { tmp[i] = q; });
+                    cta_spmv(A, v_n, scratch, [&](int r, double a) { vn_m[r] = yk[r] != 0.0 ? a : 0.0; });
+                    cta_spmv(AT, v_m, scratch,
+                             [&](int i, double at) { vn_n[i] = zk[i] == 0.0 ? tmp[i] + at : 0.0; });
+                } else {
+                    cta_spmv(Q, v_n, scratch, [&](int i, double q) { vn_n[i] = zk[i] == 0.0 ? q : 0.0; });
+                }
+                __syncthreads();
+                double al[1] = {0.0};
+                for (int i = tid; i < n; i += kBT) al[0] += v_n[i] * vn_n[i];
+                for (int r = tid; r < m; r += kBT) al[0] += v_m[r] * vn_m[r];
+                cta_allreduce<1>(al, ops1, s_red, s_out);
+                const double alpha = al[0];
+                double bn[1] = {0.0};
+                for (int i = tid; i < n; i += kBT) {
+                    const double t = vn_n[i] - alpha * v_n[i] - beta * vo_n[i];
+                    vn_n[i] = t;
+                    bn[0] += t * t;
+                }
+                for (int r = tid; r < m; r += kBT) {
+                    const double t = vn_m[r] - alpha * v_m[r] - beta * vo_m[r];
+                    vn_m[r] = t;
+                    bn[0] += t * t;
+                }
+                cta_allreduce<1>(bn, ops1, s_red, s_out);
+                const double beta_new = sqrt(bn[0]);
+                // Givens QR of the new tridiagonal column
+                const double r1h = c * alpha - c_old * s * beta;
+                const double r1 = sqrt(r1h * r1h + beta_new * beta_new);
+                const double r2 = s * alpha + c_old * c * beta;
+                const double r3 = s_old * beta;
+                const double c_new = r1 > 0.0 ? r1h / r1 : 1.0;
+                const double s_new = r1 > 0.0 ? beta_new / r1 : 0.0;
+                const double inv_r1 = r1 > 0.0 ? 1.0 / r1 : 0.0;
+                const double step = c_new * eta;
+                const double inv_b = beta_new > 0.0 ? 1.0 / beta_new : 0.0;
+                for (int i = tid; i < n; i += kBT) {
+                    const double wn = (v_n[i] - r3 * wo_n[i] - r2 * w_n[i]) * inv_r1;
+                    wn_n[i] = wn;
+                    sol_n[i] += step * wn;
+                    vn_n[i] *= inv_b;
+                }
+                for (int r = tid; r < m; r += kBT) {
+                    const double wn = (v_m[r] - r3 * wo_m[r] - r2 * w_m[r]) * inv_r1;
+                    wn_m[r] = wn;
+                    sol_m[r] += step * wn;
+                    vn_m[r] *= inv_b;
+                }
+                eta = -s_new * eta;
+                __syncthreads();
+                // rotate v_old <- v <- v_new and w_old <- w <- w_new
+                double *t0 = vo_n;
+                vo_n = v_n;
+                v_n = vn_n;
+                vn_n = t0;
+                t0 = vo_m;
+                vo_m = v_m;
+                v_m = vn_m;
+                vn_m = t0;
+                t0 = wo_n;
+                wo_n = w_n;
+                w_n = wn_n;
+                wn_n = t0;
+                t0 = wo_m;
+                wo_m = w_m;
+                w_m = wn_m;
+                wn_m = t0;
+                beta = beta_new;
+                c_old = c;
+                c = c_new;
+                s_old = s;
+                s = s_new;
+                if (fabs(eta) <= B.tol * beta0 || beta_new == 0.0) {
+                    ++it;
+                    break;
+                }
+            }
+        }
+        for (int i = tid; i < n; i += kBT) B.lam_x[I.var + i] = sol_n[i] / cn[i];
+        for (int r = tid; r < m; r += kBT) B.lam_y[I.row + r] = sol_m[r] / rn[r];
+        if (tid == 0) {
+            B.iters[k] = it;
+            B.relres[k] = beta0 > 0.0 ? fabs(eta) / beta0 : 0.0;
         }
         __syncthreads();
     }
@@ -1024,6 +1214,14 @@ struct HPRQPBatch {
     hpr::BatchArgs args{};
     double last_ms = 0.0;
     bool solved = false;
+    // the caller's CSR index arrays of Q and A (the adjoint writes one value per caller nonzero)
+    std::vector<size_t> q_rp_in, q_ci_in, a_rp_in, a_ci_in;
+    // adjoint buffers, allocated by the first hprqp_batch_backward
+    double *adj_gx = nullptr, *adj_gy = nullptr, *adj_lx = nullptr, *adj_ly = nullptr, *adj_rel = nullptr;
+    double *adj_ws = nullptr;
+    int *adj_it = nullptr, *adj_counter = nullptr;
+    size_t adj_ws_count = 0;
+    double last_adjoint_ms = 0.0;
     // host copies of the preprocessed models (kept for the adjoint)
     std::vector<HPRQPModel> models;
 };
@@ -1124,6 +1322,10 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
     b->models.resize(K);
     for (auto &mm : b->models) model_init(&mm);
     b->kept_rows.resize(K);
+    b->q_rp_in.assign(Q->row_ptr, Q->row_ptr + Q->nrow + 1);
+    b->q_ci_in.assign(Q->col_ind, Q->col_ind + Q->nnz);
+    b->a_rp_in.assign(A->row_ptr, A->row_ptr + A->nrow + 1);
+    b->a_ci_in.assign(A->col_ind, A->col_ind + A->nnz);
     // ---- per-instance build + preprocess (the single-QP builder), threaded
     std::vector<HPRQPStatus> st_k(K, HPRQP_STATUS_OK);
     const unsigned nth = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
@@ -1264,7 +1466,8 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
         (st = balloc(b, &G.y, h_AL.size())) || (st = balloc(b, &G.status, K)) || (st = balloc(b, &G.iters, K)) ||
         (st = balloc(b, &G.pobj, K)) || (st = balloc(b, &G.resid, K)) || (st = balloc(b, &G.gap, K)) ||
         (st = balloc(b, &G.restarts, K)) || (st = balloc(b, &G.active_x, h_c.size())) ||
-        (st = balloc(b, &G.active_r, h_AL.size())))
+        (st = balloc(b, &G.active_r, h_AL.size())) || (st = balloc(b, &G.col_norm_out, h_c.size())) ||
+        (st = balloc(b, &G.row_norm_out, h_AL.size())))
         return fail(st);
     // largest instances first
     std::vector<int> order(K);
@@ -1430,6 +1633,176 @@ HPRQPStatus hprqp_batch_get_results(const HPRQPBatch *b, int *status, size_t *it
     }
     return HPRQP_STATUS_OK;
 }
+
+HPRQPStatus hprqp_batch_backward(HPRQPBatch *b, const double *grad_x, const double *grad_y, double tol,
+                                 HPRQPBatchGradients *out)
+{
+    using namespace hpr;
+    if (!b || !grad_x || !out) return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (!b->solved) {
+        fprintf(stderr, "hprqp-b200: hprqp_batch_backward needs a completed hprqp_batch_solve\n");
+        return HPRQP_STATUS_INVALID_ARGUMENT;
+    }
+    if (!(tol > 0.0)) tol = 1e-12;
+    B_CK(cudaSetDevice(b->device));
+    const size_t K = b->K, N = b->total_n, M = b->total_m;
+    BatchArgs &G = b->args;
+    HPRQPStatus st;
+    // ---- device buffers (first call only)
+    const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
+    const size_t lz_bytes = (size_t)kAdjLanczos * (na + ma) * sizeof(double);
+    const int lanczos_smem = kScratchBytes + lz_bytes <= kSmemLimit;
+    const size_t smem = kScratchBytes + (lanczos_smem ? lz_bytes : 0);
+    B_CK(cudaFuncSetAttribute(k_batch_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_adjoint, kBT, smem));
+    const int grid = std::max(1, std::min((int)K, b->num_sms * std::max(per_sm, 1)));
+    const size_t stride = kAdjGlobalN * na + kAdjGlobalM * ma + (lanczos_smem ? 0 : (size_t)kAdjLanczos * (na + ma));
+    if (!b->adj_gx) {
+        if ((st = balloc(b, &b->adj_gx, N)) || (st = balloc(b, &b->adj_gy, M)) || (st = balloc(b, &b->adj_lx, N)) ||
+            (st = balloc(b, &b->adj_ly, M)) || (st = balloc(b, &b->adj_rel, K)) || (st = balloc(b, &b->adj_it, K)) ||
+            (st = balloc(b, &b->adj_counter, 1)))
+            return st;
+    }
+    if (b->adj_ws_count < stride * (size_t)grid) {
+        if ((st = balloc(b, &b->adj_ws, stride * (size_t)grid))) return st;
+        b->adj_ws_count = stride * (size_t)grid;
+    }
+    // ---- loss gradients in the device packing (rows: the rows kept by preprocessing)
+    std::vector<double> gy_kept;
+    if (grad_y) {
+        gy_kept.assign(std::max<size_t>(M, 1), 0.0);
+        for (size_t k = 0; k < K; ++k) {
+            const auto &kr = b->kept_rows[k];
+            for (size_t r = 0; r < kr.size(); ++r) gy_kept[b->inst[k].row + r] = grad_y[b->row_off[k] + kr[r]];
+        }
+        B_CK(cudaMemcpyAsync(b->adj_gy, gy_kept.data(), M * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    }
+    std::vector<double> gx_dev(std::max<size_t>(N, 1), 0.0);
+    for (size_t k = 0; k < K; ++k)
+        memcpy(&gx_dev[b->inst[k].var], grad_x + b->var_off[k], (size_t)b->inst[k].n * sizeof(double));
+    B_CK(cudaMemcpyAsync(b->adj_gx, gx_dev.data(), N * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    B_CK(cudaMemsetAsync(b->adj_counter, 0, sizeof(int), b->stream));
+    AdjArgs A{};
+    A.K = (int)K;
+    A.inst = G.inst;
+    A.order = G.order;
+    A.counter = b->adj_counter;
+    A.q_rp = G.q_rp;
+    A.q_ci = G.q_ci;
+    A.a_rp = G.a_rp;
+    A.a_ci = G.a_ci;
+    A.at_rp = G.at_rp;
+    A.at_ci = G.at_ci;
+    A.q_v = G.q_v;
+    A.a_v = G.a_v;
+    A.at_v = G.at_v;
+    A.col_norm = G.col_norm_out;
+    A.row_norm = G.row_norm_out;
+    A.z = G.z;
+    A.y = G.y;
+    A.gx = b->adj_gx;
+    A.gy = grad_y ? b->adj_gy : nullptr;
+    A.lam_x = b->adj_lx;
+    A.lam_y = b->adj_ly;
+    A.iters = b->adj_it;
+    A.relres = b->adj_rel;
+    A.tol = tol;
+    A.maxit_factor = 4;
+    A.ws = b->adj_ws;
+    A.ws_stride = stride;
+    A.nmax = G.nmax;
+    A.mmax = G.mmax;
+    A.lanczos_smem = lanczos_smem;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, b->stream);
+    k_batch_adjoint<<<grid, kBT, smem, b->stream>>>(A);
+    count_launch();
+    cudaEventRecord(e1, b->stream);
+    cudaError_t err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    B_CK(err);
+    B_CK(cudaGetLastError());
+    b->last_adjoint_ms = ms;
+    // ---- lambda, mu and the solution back on the host (device packing)
+    std::vector<double> lx(std::max<size_t>(N, 1)), ly(std::max<size_t>(M, 1)), x(std::max<size_t>(N, 1)),
+        z(std::max<size_t>(N, 1)), y(std::max<size_t>(M, 1)), rel(K);
+    std::vector<int> its(K);
+    B_CK(cudaMemcpyAsync(lx.data(), b->adj_lx, N * 8, cudaMemcpyDeviceToHost, b->stream));
+    B_CK(cudaMemcpyAsync(ly.data(), b->adj_ly, M * 8, cudaMemcpyDeviceToHost, b->stream));
+    B_CK(cudaMemcpyAsync(x.data(), G.x, N * 8, cudaMemcpyDeviceToHost, b->stream));
+    B_CK(cudaMemcpyAsync(z.data(), G.z, N * 8, cudaMemcpyDeviceToHost, b->stream));
+    B_CK(cudaMemcpyAsync(y.data(), G.y, M * 8, cudaMemcpyDeviceToHost, b->stream));
+    B_CK(cudaMemcpyAsync(rel.data(), b->adj_rel, K * 8, cudaMemcpyDeviceToHost, b->stream));
+    B_CK(cudaMemcpyAsync(its.data(), b->adj_it, K * 4, cudaMemcpyDeviceToHost, b->stream));
+    B_CK(cudaStreamSynchronize(b->stream));
+    if (out->minres_iters) memcpy(out->minres_iters, its.data(), K * sizeof(int));
+    if (out->minres_relres) memcpy(out->minres_relres, rel.data(), K * sizeof(double));
+    // ---- gradient assembly, per instance on host threads (caller's packing)
+    const unsigned nth = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    auto worker = [&](unsigned tix) {
+        std::vector<double> qlam, atmu, mu_orig, y_orig;
+        for (size_t k = tix; k < K; k += nth) {
+            const HPRQPModel &Mk = b->models[k];
+            const BInst &I = b->inst[k];
+            const size_t n = Mk.Q.ncol, m = Mk.A.nrow, v0 = b->var_off[k], r0 = b->row_off[k];
+            const size_t m_orig = b->row_off[k + 1] - r0;
+            const double *lam = lx.data() + I.var, *mu = ly.data() + I.row, *xk = x.data() + I.var;
+            const double *zk = z.data() + I.var, *yk = y.data() + I.row, *gk = grad_x + v0;
+            // Q lam and A' mu with the preprocessed (symmetrised, unscaled) model
+            qlam.assign(n, 0.0);
+            atmu.assign(n, 0.0);
+            for (size_t i = 0; i < n; ++i)
+                for (size_t e = Mk.Q.row_ptr[i]; e < Mk.Q.row_ptr[i + 1]; ++e)
+                    qlam[i] += Mk.Q.values[e] * lam[Mk.Q.col_ind[e]];
+            for (size_t r = 0; r < m; ++r)
+                for (size_t e = Mk.A.row_ptr[r]; e < Mk.A.row_ptr[r + 1]; ++e)
+                    atmu[Mk.A.col_ind[e]] += Mk.A.values[e] * mu[r];
+            for (size_t i = 0; i < n; ++i) {
+                if (out->dc) out->dc[v0 + i] = -lam[i];
+                const double db = gk[i] - qlam[i] - atmu[i];
+                if (out->dl) out->dl[v0 + i] = zk[i] > 0.0 ? db : 0.0;
+                if (out->du) out->du[v0 + i] = zk[i] < 0.0 ? db : 0.0;
+            }
+            mu_orig.assign(m_orig, 0.0);
+            y_orig.assign(m_orig, 0.0);
+            const auto &kr = b->kept_rows[k];
+            for (size_t r = 0; r < kr.size(); ++r) {
+                mu_orig[kr[r]] = mu[r];
+                y_orig[kr[r]] = yk[r];
+            }
+            for (size_t r = 0; r < m_orig; ++r) {
+                if (out->dAL) out->dAL[r0 + r] = y_orig[r] > 0.0 ? mu_orig[r] : 0.0;
+                if (out->dAU) out->dAU[r0 + r] = y_orig[r] < 0.0 ? mu_orig[r] : 0.0;
+            }
+            // caller's Q entry (i, j) enters (Q + Q')/2 at (i, j) and (j, i)
+            if (out->dQ_values)
+                for (size_t i = 0; i < n; ++i)
+                    for (size_t e = b->q_rp_in[v0 + i]; e < b->q_rp_in[v0 + i + 1]; ++e) {
+                        const size_t j = b->q_ci_in[e] - v0;
+                        out->dQ_values[e] = -0.5 * (lam[i] * xk[j] + lam[j] * xk[i]);
+                    }
+            // caller's A entry (r, j)
+            if (out->dA_values)
+                for (size_t r = 0; r < m_orig; ++r)
+                    for (size_t e = b->a_rp_in[r0 + r]; e < b->a_rp_in[r0 + r + 1]; ++e) {
+                        const size_t j = b->a_ci_in[e] - v0;
+                        out->dA_values[e] = -mu_orig[r] * xk[j] + lam[j] * y_orig[r];
+                    }
+        }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nth; ++t) th.emplace_back(worker, t);
+    for (auto &t : th) t.join();
+    return HPRQP_STATUS_OK;
+}
+
+double hprqp_batch_last_backward_ms(const HPRQPBatch *b) { return b ? b->last_adjoint_ms : 0.0; }
 
 void hprqp_batch_destroy(HPRQPBatch *b)
 {

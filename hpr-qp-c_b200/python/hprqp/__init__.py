@@ -489,8 +489,18 @@ def model_arrays(model: Model):
                 obj_constant=float(ms.obj_constant))
 
 
+def __getattr__(name):
+    """``hprqp.QPFunction`` / ``hprqp.QPLayer``: the differentiable batched
+    layer (imported on first use so that torch stays optional)."""
+    if name in ("QPFunction", "QPLayer"):
+        from . import torch_layer
+
+        return getattr(torch_layer, name)
+    raise AttributeError(f"module 'hprqp' has no attribute {name!r}")
+
+
 __all__ = [
-    "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
+    "QPFunction", "QPLayer", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
     "STATUS_ALLOCATION_FAILED", "STATUS_CONTINUE", "STATUS_INVALID_ARGUMENT", "STATUS_MAX_ITER",
     "STATUS_NOT_IMPLEMENTED", "STATUS_OK", "STATUS_OPTIMAL", "STATUS_TIME_LIMIT", "build_from_mps",
     "build_from_QAbc", "build_from_qabc", "build_from_instance", "gpu_backend_available", "optimize",

@@ -13,6 +13,12 @@ from . import _MatrixCSR, _lib, _raise_for_status, c_double_p, c_size_p
 _configured = False
 
 
+class BatchGradients(ctypes.Structure):
+    _fields_ = [(name, ctypes.POINTER(ctypes.c_double)) for name in ("dc", "dl", "du", "dAL", "dAU", "dQ_values",
+                                                                     "dA_values")] + \
+               [("minres_iters", ctypes.POINTER(ctypes.c_int)), ("minres_relres", ctypes.POINTER(ctypes.c_double))]
+
+
 class BatchParams(ctypes.Structure):
     _fields_ = [("stoptol", ctypes.c_double), ("max_iter", ctypes.c_size_t), ("time_limit", ctypes.c_double),
                 ("check_iter", ctypes.c_size_t), ("print_frequency", ctypes.c_int), ("use_scaling", ctypes.c_int),
@@ -35,6 +41,10 @@ def _configure():
     lib.hprqp_batch_last_solve_ms.restype = ctypes.c_double
     lib.hprqp_batch_get_results.argtypes = [vp, ctypes.POINTER(ctypes.c_int), c_size_p, c_double_p, c_double_p,
                                             c_double_p, c_double_p, c_double_p, c_double_p, c_double_p]
+    lib.hprqp_batch_backward.argtypes = [vp, c_double_p, c_double_p, ctypes.c_double,
+                                         ctypes.POINTER(BatchGradients)]
+    lib.hprqp_batch_last_backward_ms.argtypes = [vp]
+    lib.hprqp_batch_last_backward_ms.restype = ctypes.c_double
     lib.hprqp_batch_destroy.argtypes = [vp]
     lib.hprqp_batch_destroy.restype = None
     _configured = True
@@ -129,6 +139,22 @@ class BatchResult:
     solve_ms: float
 
 
+@dataclass
+class Gradients:
+    """dL/d(problem data) from hprqp_batch_backward, packed like the inputs
+    (dQ / dA: one value per nonzero of the caller's Q / A)."""
+    dc: np.ndarray
+    dl: np.ndarray
+    du: np.ndarray
+    dAL: np.ndarray
+    dAU: np.ndarray
+    dQ: np.ndarray
+    dA: np.ndarray
+    minres_iters: np.ndarray
+    minres_relres: np.ndarray
+    backward_ms: float
+
+
 class Batch:
     """Device-resident batch: create once, solve many times."""
 
@@ -182,6 +208,32 @@ class Batch:
         _raise_for_status(st, "hprqp_batch_get_results")
         return BatchResult(status, it.astype(np.int64), obj, res, gap, x[:self.n], y[:self.m], z[:self.n],
                            w[:self.n], float(_lib().hprqp_batch_last_solve_ms(self._handle)))
+
+    def backward(self, grad_x, grad_y=None, tol: float = 1e-12) -> Gradients:
+        """Implicit-differentiation adjoint of the last solve (one MINRES
+        solve per instance on the device); see hprqp_batch_backward."""
+        gx = np.ascontiguousarray(np.broadcast_to(np.asarray(grad_x, np.float64), (self.n,)))
+        gy = None if grad_y is None else np.ascontiguousarray(np.broadcast_to(np.asarray(grad_y, np.float64),
+                                                                               (self.m,)))
+        p = self.packed
+        n1, m1 = max(self.n, 1), max(self.m, 1)
+        out = {k: np.zeros(v) for k, v in (("dc", n1), ("dl", n1), ("du", n1), ("dAL", m1), ("dAU", m1),
+                                           ("dQ_values", max(len(p.q_data), 1)),
+                                           ("dA_values", max(len(p.a_data), 1)))}
+        its = np.zeros(self.K, np.int32)
+        rel = np.zeros(self.K)
+        g = BatchGradients(**{k: v.ctypes.data_as(c_double_p) for k, v in out.items()},
+                           minres_iters=its.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                           minres_relres=rel.ctypes.data_as(c_double_p))
+        gx_buf = gx if self.n else np.zeros(1)
+        gy_buf = None if gy is None else (gy if self.m else np.zeros(1))
+        st = _lib().hprqp_batch_backward(self._handle, gx_buf.ctypes.data_as(c_double_p),
+                                         None if gy_buf is None else gy_buf.ctypes.data_as(c_double_p),
+                                         float(tol), ctypes.byref(g))
+        _raise_for_status(st, "hprqp_batch_backward")
+        return Gradients(out["dc"][:self.n], out["dl"][:self.n], out["du"][:self.n], out["dAL"][:self.m],
+                         out["dAU"][:self.m], out["dQ_values"][:len(p.q_data)], out["dA_values"][:len(p.a_data)],
+                         its, rel, float(_lib().hprqp_batch_last_backward_ms(self._handle)))
 
     def split(self, vec: np.ndarray, kind: str) -> List[np.ndarray]:
         off = self.packed.var_offsets if kind == "x" else self.packed.row_offsets

@@ -232,6 +232,31 @@ def config4(count: int = 256, start: int = 0) -> List[QPInstance]:
     return [config4_instance(start + i) for i in range(count)]
 
 
+def adjoint_case(instance: int, n: int = 60, m: int = 30) -> QPInstance:
+    """Small QP with bounds tight enough that a share of variables and rows
+    end at a bound (for differentiation tests): box [-0.5, 0.5] on most
+    variables, a few free variables, equality, ranged and one-sided rows."""
+    rng = np.random.default_rng(SEED_BASE + 5000 + instance)
+    r, c = _uniform_pattern(rng, m, n, int(0.15 * m * n))
+    A = _csr_from_coo(m, n, r, c, rng.standard_normal(len(r)))
+    Q = _gram_plus_ridge(rng, n, n // 2, 0.1, 0.1)
+    x0 = rng.uniform(-0.3, 0.3, n)
+    ax = A.to_scipy() @ x0
+    n_eq = m // 4
+    AL = ax - rng.uniform(0.0, 0.5, m)
+    AU = ax + rng.uniform(0.0, 0.5, m)
+    AL[:n_eq] = AU[:n_eq] = ax[:n_eq]
+    one_sided = rng.random(m) < 0.25
+    one_sided[:n_eq] = False
+    AU[one_sided] = np.inf
+    l = np.full(n, -0.5)
+    u = np.full(n, 0.5)
+    free = rng.random(n) < 0.1
+    l[free], u[free] = -np.inf, np.inf
+    cvec = 3.0 * rng.standard_normal(n)
+    return QPInstance(Q, A, cvec, AL, AU, l, u, 0.0, f"adjoint_{instance}")
+
+
 def tiny_cases() -> List[QPInstance]:
     """Hand-written models mirroring the reference's test fixtures
     (tests/test_support.c:79-268 of the reference project): dense-list form

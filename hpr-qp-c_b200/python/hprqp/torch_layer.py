@@ -1,0 +1,94 @@
+"""Differentiable batched QP layer for PyTorch.
+
+    min_x  1/2 x'Qx + c'x   s.t.  AL <= Ax <= AU,  l <= x <= u
+
+for a batch of QPs that share one sparsity structure (given once as a
+:class:`hprqp.batch.Packed`), with the numeric data passed as tensors.  The
+forward pass runs the batched persistent solver (hprqp_batch_solve); the
+backward pass runs the implicit-differentiation adjoint
+(hprqp_batch_backward): one MINRES solve per instance on the active-set KKT
+system
+
+    [[Q_FF, A_RF'], [A_RF, 0]] [lam_F; mu_R] = [dL/dx_F; -dL/dy_R]
+
+(F: variables off their bounds, R: rows at a bound), then
+
+    dL/dc = -lam,  dL/dAL_r = mu_r (y_r > 0),  dL/dAU_r = mu_r (y_r < 0),
+    dL/dl_i (z_i > 0), dL/du_i (z_i < 0) = dL/dx_i - (Q lam)_i - (A' mu)_i,
+    dL/dQ_ij = -(lam_i x_j + lam_j x_i) / 2,  dL/dA_rj = -mu_r x_j + lam_j y_r.
+
+The reference (PolyU-IOR/HPR-QP-C) has no differentiable layer; this module
+is an addition.  The solve and the adjoint run on the GPU; tensors cross the
+C ABI as host float64 arrays, and results come back on the inputs' device.
+"""
+from __future__ import annotations
+
+from dataclasses import replace
+from typing import Optional
+
+import numpy as np
+import torch
+
+from .batch import Batch, Packed
+
+
+def _np(t: torch.Tensor) -> np.ndarray:
+    return t.detach().to("cpu", torch.float64).contiguous().numpy()
+
+
+class QPFunction(torch.autograd.Function):
+    """``QPFunction.apply(structure, solve_kw, backward_tol, q_data, a_data,
+    c, AL, AU, l, u) -> (x, y)``; ``structure`` fixes offsets and CSR index
+    arrays, the tensors give the values in the same packing."""
+
+    @staticmethod
+    def forward(ctx, structure: Packed, solve_kw: dict, backward_tol: float, q_data, a_data, c, AL, AU, l, u):
+        packed = replace(structure, q_data=_np(q_data), a_data=_np(a_data), c=_np(c), AL=_np(AL), AU=_np(AU),
+                         l=_np(l), u=_np(u))
+        kw = dict(solve_kw)
+        batch = Batch(packed, device_number=kw.pop("device_number", 0))
+        try:
+            batch.solve(**kw)
+            res = batch.results()
+        except Exception:
+            batch.close()
+            raise
+        ctx.batch = batch
+        ctx.backward_tol = backward_tol
+        ctx.device = c.device
+        ctx.status = res.status
+        x = torch.from_numpy(res.x.copy()).to(c.device)
+        y = torch.from_numpy(res.y.copy()).to(c.device)
+        return x, y
+
+    @staticmethod
+    def backward(ctx, gx, gy):
+        batch: Optional[Batch] = getattr(ctx, "batch", None)
+        if batch is None:
+            raise RuntimeError("hprqp QPFunction: backward called twice (retain_graph is not supported)")
+        try:
+            g = batch.backward(_np(gx) if gx is not None else np.zeros(batch.n),
+                               _np(gy) if gy is not None else None, tol=ctx.backward_tol)
+        finally:
+            batch.close()
+            ctx.batch = None
+        dev = ctx.device
+        t = lambda a: torch.from_numpy(a.copy()).to(dev)  # noqa: E731
+        return (None, None, None, t(g.dQ), t(g.dA), t(g.dc), t(g.dAL), t(g.dAU), t(g.dl), t(g.du))
+
+
+class QPLayer(torch.nn.Module):
+    """Batched QP layer.  ``structure`` fixes the offsets and the CSR index
+    arrays of Q and A (its numeric arrays are ignored); ``forward`` takes the
+    data tensors packed the same way and returns ``(x, y)``.  Solver
+    parameters (``stoptol``, default 1e-8, ``max_iter``, ...) are passed as
+    keywords."""
+
+    def __init__(self, structure: Packed, backward_tol: float = 1e-12, **solve_kw):
+        super().__init__()
+        self.structure = structure
+        self.backward_tol = backward_tol
+        self.solve_kw = {"stoptol": 1e-8, **solve_kw}
+
+    def forward(self, q_data, a_data, c, AL, AU, l, u):
+        return QPFunction.apply(self.structure, self.solve_kw, self.backward_tol, q_data, a_data, c, AL, AU, l, u)

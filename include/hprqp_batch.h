@@ -61,6 +61,41 @@ size_t hprqp_batch_num_instances(const HPRQPBatch *batch);
 HPRQPStatus hprqp_batch_get_results(const HPRQPBatch *batch, int *status, size_t *iter, double *primal_obj,
                                     double *residual, double *gap, double *x, double *y, double *z, double *w);
 
+/* Gradients of a scalar loss L(x*, y*) with respect to the problem data, by
+ * implicit differentiation of the KKT conditions on the active set of the
+ * last hprqp_batch_solve: variables with z != 0 sit at a bound (z > 0 lower,
+ * z < 0 upper), rows with y != 0 at a bound (y > 0 lower, y < 0 upper);
+ * strict complementarity is assumed.  Any output pointer may be NULL.
+ * Packing as in hprqp_batch_create:
+ *   dc, dl, du     total variables;  dAL, dAU  total rows (the caller's rows;
+ *                  an equality row reports its whole gradient on the active
+ *                  side, so dAL + dAU is the gradient of moving both sides);
+ *   dQ_values      one value per nonzero of the caller's Q (the solver uses
+ *                  (Q + Q')/2, so entry (i,j) gets -(lam_i x_j + lam_j x_i)/2);
+ *   dA_values      one value per nonzero of the caller's A;
+ *   minres_iters, minres_relres   per instance. */
+typedef struct HPRQPBatchGradients {
+    double *dc;
+    double *dl;
+    double *du;
+    double *dAL;
+    double *dAU;
+    double *dQ_values;
+    double *dA_values;
+    int *minres_iters;
+    double *minres_relres;
+} HPRQPBatchGradients;
+
+/* grad_x: dL/dx* (total variables); grad_y: dL/dy* (total rows) or NULL;
+ * tol: relative MINRES residual (<= 0 selects 1e-12).  The adjoint systems
+ * are solved on the device, one instance per CTA; the gradients are
+ * assembled on the host. */
+HPRQPStatus hprqp_batch_backward(HPRQPBatch *batch, const double *grad_x, const double *grad_y, double tol,
+                                 HPRQPBatchGradients *gradients);
+
+/* Device time of the last adjoint kernel, milliseconds. */
+double hprqp_batch_last_backward_ms(const HPRQPBatch *batch);
+
 void hprqp_batch_destroy(HPRQPBatch *batch);
 
 /* One-call form: create + solve + get_results + destroy. */

@@ -207,6 +207,55 @@ class OracleModel:
         return dict(err_rp=out[0], err_rd=out[1], gap=out[2], primal_obj=out[3], dual_obj=out[4], kkt=out[5])
 
 
+def kkt_adjoint_dense(inst, x, y, z, grad_x, grad_y=None):
+    """Dense FP64 implicit-differentiation adjoint of a QP solution.
+
+    The reference (PolyU-IOR/HPR-QP-C) has no adjoint; this is the checker
+    for the device MINRES adjoint.  Its sign conventions are the reference's
+    KKT conditions (src/gpu/residuals.cu: Qx + c - A'y - z = 0, y_r > 0 at the
+    lower row bound, z_i > 0 at the lower variable bound).  Active sets:
+    F = {i : z_i == 0}, R = {r : y_r != 0}.  Solves
+    [[Q_FF, A_RF'], [A_RF, 0]] [lam_F; mu_R] = [g_F; -gy_R] with numpy's
+    dense solver (least squares when singular) and returns every gradient.
+    ``y``/``grad_y`` cover all of the instance's rows (removed rows: y = 0).
+    """
+    Q = inst.Q.dense()
+    Q = 0.5 * (Q + Q.T)
+    A = inst.A.dense()
+    n, m = Q.shape[0], A.shape[0]
+    x, y, z = (np.asarray(v, np.float64) for v in (x, y, z))
+    gx = np.asarray(grad_x, np.float64)
+    gy = np.zeros(m) if grad_y is None else np.asarray(grad_y, np.float64)
+    F = np.nonzero(z == 0.0)[0]
+    R = np.nonzero(y != 0.0)[0]
+    nf, nr = len(F), len(R)
+    K = np.zeros((nf + nr, nf + nr))
+    K[:nf, :nf] = Q[np.ix_(F, F)]
+    K[:nf, nf:] = A[np.ix_(R, F)].T
+    K[nf:, :nf] = A[np.ix_(R, F)]
+    rhs = np.concatenate([gx[F], -gy[R]])
+    try:
+        sol = np.linalg.solve(K, rhs)
+    except np.linalg.LinAlgError:
+        sol = np.linalg.lstsq(K, rhs, rcond=None)[0]
+    lam = np.zeros(n)
+    mu = np.zeros(m)
+    lam[F] = sol[:nf]
+    mu[R] = sol[nf:]
+    db = gx - Q @ lam - A.T @ mu
+    qi, qj = _coo(inst.Q)
+    ai, aj = _coo(inst.A)
+    return dict(lam=lam, mu=mu, dc=-lam, dl=np.where(z > 0.0, db, 0.0), du=np.where(z < 0.0, db, 0.0),
+                dAL=np.where(y > 0.0, mu, 0.0), dAU=np.where(y < 0.0, mu, 0.0),
+                dQ=-0.5 * (lam[qi] * x[qj] + lam[qj] * x[qi]), dA=-mu[ai] * x[aj] + lam[aj] * y[ai])
+
+
+def _coo(csr):
+    indptr = np.asarray(csr.indptr, np.int64)
+    rows = np.repeat(np.arange(len(indptr) - 1), np.diff(indptr))
+    return rows, np.asarray(csr.indices, np.int64)
+
+
 def matvec(indptr, indices, data, x):
     indptr_a, ip = _sz(indptr)
     indices_a, ii = _sz(indices if len(indices) else np.zeros(1))
