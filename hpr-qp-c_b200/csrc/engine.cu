@@ -1697,6 +1697,8 @@ static HPRQPStatus spmv_standalone(size_t nrow, size_t ncol, size_t nnz, const s
     double total_ms = 0.0;
     // matrices smaller than 2 x L2 would be timed from L2: evict them first
     const bool do_flush = nnz * 12 + nrow * 4 < ((size_t)256 << 20);
+    // one untimed launch first (module loading, first-touch of the buffers)
+    launch_rb(e, M, dx, ep);
     for (int r = 0; r < reps; ++r) {
         if (do_flush) cudaMemsetAsync(flush, r & 0xff, flush_bytes, e->stream);
         cudaEventRecord(ev0, e->stream);

@@ -1,23 +1,26 @@
-// Warp-tiled CSR SpMV with a fused per-row epilogue (sm_100a, FP64).
+// Tiled CSR SpMV with a fused per-row epilogue (sm_100a, FP64).
 //
 // Every HPR kernel is "y = M x, then an elementwise update of row i that
 // consumes y_i" (the reference fuses the same way with a thread-per-row dot,
 // src/gpu/iteration.cu:282-697).  The cost of y = M x on B200 is the latency
-// of the x[col] gathers (x lives in L2, the matrix streams from HBM), so the
-// kernel is built to keep as many independent loads in flight as possible:
+// of the matrix stream from HBM and of the x[col] gathers from L2, so the
+// kernel keeps many independent loads in flight and never lets a short or
+// long row idle a lane:
 //
-//   * each matrix is cut once, at setup, into warp tiles of up to 32
-//     consecutive rows; a tile also fixes its lane-group width G (1..32), a
-//     power of two near a quarter of the tile's mean row length, so each
-//     lane of a group adds a few entries of its row;
-//   * a warp walks its tile in 32/G-row passes; inside a row, a lane issues
-//     four independent value/column/x loads per step (values and indices are
-//     read once, with evict-first hints so they do not displace x in L2);
-//   * the row sums are shuffled so that lane i holds row i, and the
-//     epilogue runs on all 32 lanes for 32 consecutive rows: coalesced;
-//   * rows longer than kLongRow are cut into kChunk-entry chunks, one warp
-//     per chunk; a second tiny kernel adds a row's chunk partials in order
-//     and runs its epilogue;
+//   * each matrix is cut once, at setup, into warp tiles: consecutive rows,
+//     at most kTileRows of them and at most kTileCap entries in total (a row
+//     longer than kTileCap is cut into kTileCap-entry chunks, one warp per
+//     chunk, and a second tiny kernel adds its chunk partials in order);
+//   * a warp streams its tile's entries as flat 256-entry windows: eight
+//     coalesced index/value loads per lane, issued for the next window
+//     before the x gathers of the current one are consumed;
+//   * the 256 products go to shared memory and are summed per row by a
+//     segmented scan (rows may start and end anywhere in a window; head
+//     flags come from the tile's row starts, staged in shared memory, and a
+//     carry links windows), so every lane does the same work whatever the
+//     row lengths are;
+//   * the row sums are collected in shared memory and the epilogue runs
+//     after the tile, lane i on rows i, i + 32: coalesced;
 //   * reductions requested by an epilogue are folded per CTA in a fixed
 //     order, so results are bit-reproducible run to run.
 #pragma once
@@ -31,11 +34,13 @@ namespace hpr {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kLongRow = 4096;  // rows longer than this are chunked
-constexpr int kChunk = 2048;    // entries per chunk of a long row
-constexpr int kSoloRow = 256;   // rows at least this long get a tile of their own
+constexpr int kTileRows = 64;   // rows per warp tile (two per lane)
+constexpr int kTileCap = 1024;  // entries per warp tile; longer rows are chunked
+constexpr int kChunk = kTileCap;  // entries per chunk of a long row
+constexpr int kSpmvWinU = 8;  // entries per lane per window
+constexpr int kSpmvWin = 32 * kSpmvWinU;  // entries per window
 #ifndef HPR_SPMV_MIN_BLOCKS
-#define HPR_SPMV_MIN_BLOCKS 4  // CTAs per SM the register budget must allow
+#define HPR_SPMV_MIN_BLOCKS 3  // CTAs per SM the register budget must allow
 #endif
 
 struct DCsr {
@@ -43,7 +48,7 @@ struct DCsr {
     int *rp = nullptr;
     int *ci = nullptr;
     double *v = nullptr;
-    int4 *tiles = nullptr;  // {r0, r1, G, 0}
+    int4 *tiles = nullptr;  // {r0, r1, entries, 0}
     int ntiles = 0;
     int4 *chunks = nullptr;  // {row, k0, k1, slot}
     int nchunks = 0;
@@ -51,7 +56,7 @@ struct DCsr {
     int nlong = 0;
     double *chunk_partial = nullptr;
     int *err = nullptr;
-    int grid_main = 0;   // CTAs of k_spmv (8 tiles each)
+    int grid_main = 0;   // CTAs of k_spmv (one tile per warp)
     int grid_chunk = 0;  // CTAs of k_chunks (8 chunks each)
     int grid_long = 0;   // CTAs of k_long_epi
     int npart() const { return grid_main + grid_long; }
@@ -135,6 +140,114 @@ __device__ __forceinline__ double row_dot(const DCsr &M, const double *__restric
     return (s0 + s1) + (s2 + s3);
 }
 
+// padded shared-memory slot of window entry i (conflict-free for both the
+// strided writes and the lane-contiguous reads of the segmented scan)
+__device__ __forceinline__ int win_slot(int i) { return i + (i >> 3); }
+
+// Row sums of one warp tile (rows r0 .. r0 + nr - 1, entries k0 .. k1 - 1,
+// at most kTileRows rows and kTileCap entries) into rowsum[0 .. nr - 1].
+// rs[0 .. nr] are the tile's row starts in shared memory.
+__device__ __forceinline__ void tile_rowsums(const DCsr &M, const double *__restrict__ x, const int *rs, int nr,
+                                             double *sv, unsigned char *sh, double *rowsum)
+{
+    constexpr int KR = kTileRows / 32;
+    const int lane = threadIdx.x & 31;
+    const int k0 = rs[0], k1 = rs[nr];
+#pragma unroll
+    for (int j = 0; j < KR; ++j) {
+        const int r = lane + 32 * j;
+        if (r < nr) rowsum[r] = 0.0;  // empty rows keep 0
+    }
+    double carry = 0.0;
+    int c[kSpmvWinU];
+    double v[kSpmvWinU];
+#pragma unroll
+    for (int u = 0; u < kSpmvWinU; ++u) {
+        const int k = k0 + u * 32 + lane;
+        c[u] = k < k1 ? __ldcs(M.ci + k) : 0;
+        v[u] = k < k1 ? __ldcs(M.v + k) : 0.0;
+    }
+    for (int base = k0; base < k1; base += kSpmvWin) {
+        const int nb = base + kSpmvWin;
+        double p[kSpmvWinU];
+#pragma unroll
+        for (int u = 0; u < kSpmvWinU; ++u) p[u] = v[u] * __ldg(x + c[u]);
+        // next window's stream, in flight while this one is summed
+#pragma unroll
+        for (int u = 0; u < kSpmvWinU; ++u) {
+            const int k = nb + u * 32 + lane;
+            c[u] = k < k1 ? __ldcs(M.ci + k) : 0;
+            v[u] = k < k1 ? __ldcs(M.v + k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kSpmvWinU; ++u) {
+            const int i = u * 32 + lane;
+            sv[win_slot(i)] = p[u];
+            sh[i] = 0;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < KR; ++j) {
+            const int r = lane + 32 * j;
+            if (r < nr) {
+                const int a = rs[r], e = rs[r + 1];
+                if (a < e && a >= base && a < nb) sh[a - base] = 1;
+            }
+        }
+        __syncwarp();
+        // lane-contiguous segmented sums, lane 0 continuing the carried row
+        double run = lane == 0 ? carry : 0.0;
+        bool seg = false;
+#pragma unroll
+        for (int j = 0; j < kSpmvWinU; ++j) {
+            const int i = lane * kSpmvWinU + j;
+            const double q = sv[win_slot(i)];
+            if (sh[i]) {
+                run = q;
+                seg = true;
+            } else {
+                run += q;
+            }
+            p[j] = run;
+        }
+        // segmented inclusive scan of the lane tails across the warp
+        double tail = run;
+        bool tseg = seg;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const double tl = __shfl_up_sync(0xffffffffu, tail, off);
+            const bool fl = __shfl_up_sync(0xffffffffu, (int)tseg, off);
+            if (lane >= off && !tseg) {
+                tail = tl + tail;
+                tseg = fl;
+            }
+        }
+        double cin = __shfl_up_sync(0xffffffffu, tail, 1);
+        if (lane == 0) cin = 0.0;
+        __syncwarp();
+        bool h = false;
+#pragma unroll
+        for (int j = 0; j < kSpmvWinU; ++j) {
+            const int i = lane * kSpmvWinU + j;
+            h = h || sh[i];
+            if (!h) p[j] = cin + p[j];
+            sv[win_slot(i)] = p[j];
+        }
+        carry = __shfl_sync(0xffffffffu, p[kSpmvWinU - 1], 31);
+        __syncwarp();
+        // rows that end in this window
+#pragma unroll
+        for (int j = 0; j < KR; ++j) {
+            const int r = lane + 32 * j;
+            if (r < nr) {
+                const int a = rs[r], e = rs[r + 1];
+                if (a < e && e - 1 >= base && e - 1 < nb) rowsum[r] = sv[win_slot(e - 1 - base)];
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // Epilogue concept:
 //   static constexpr int NRED;  __host__ __device__ void ops(int*) const;
 //   __device__ void init(Acc&) const; row(int i, double y_i, Acc&) const;
@@ -143,26 +256,27 @@ __device__ __forceinline__ double row_dot(const DCsr &M, const double *__restric
 template <class Epi>
 __global__ void __launch_bounds__(kThreads, HPR_SPMV_MIN_BLOCKS) k_spmv(const DCsr M, const double *__restrict__ xin, const Epi epi)
 {
+    __shared__ double s_val[kWarps][kSpmvWin + kSpmvWin / 8];
+    __shared__ unsigned char s_head[kWarps][kSpmvWin];
+    __shared__ int s_rs[kWarps][kTileRows + 1];
+    __shared__ double s_row[kWarps][kTileRows];
     Acc<Epi::NRED> acc;
     epi.init(acc);
-    const int lane = threadIdx.x & 31;
-    const int t = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int t = blockIdx.x * kWarps + wid;
     if (t < M.ntiles) {
         const int4 T = M.tiles[t];
-        const int r0 = T.x, nr = T.y - T.x, G = T.z;
-        const int rpp = 32 / G;  // rows per pass
-        const int gl = lane & (G - 1), grp = lane / G;
-        const int passes = (nr + rpp - 1) / rpp;
-        double mine = 0.0;  // sum of row r0 + lane
-        for (int p = 0; p < passes; ++p) {
-            const int rr = p * rpp + grp;
-            double s = 0.0;
-            if (rr < nr) s = row_dot(M, xin, __ldg(M.rp + r0 + rr), __ldg(M.rp + r0 + rr + 1), gl, G);
-            for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            const double v = __shfl_sync(0xffffffffu, s, (lane % rpp) * G);
-            if (lane / rpp == p) mine = v;
+        const int r0 = T.x, nr = T.y - T.x;
+        int *rs = s_rs[wid];
+        for (int r = lane; r <= nr; r += 32) rs[r] = __ldg(M.rp + r0 + r);
+        __syncwarp();
+        tile_rowsums(M, xin, rs, nr, s_val[wid], s_head[wid], s_row[wid]);
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < kTileRows / 32; ++j) {
+            const int r = lane + 32 * j;
+            if (r < nr) epi.row(r0 + r, s_row[wid][r], acc);
         }
-        if (lane < nr) epi.row(r0 + lane, mine, acc);
     }
     epi.extra(acc);
     if constexpr (Epi::NRED > 0) {
@@ -231,14 +345,8 @@ struct TilePlan {
     std::vector<int2> long_rows;
 };
 
-inline int lane_group_for(long long nnz, int rows)
-{
-    const long long avg = rows > 0 ? nnz / rows : 0;
-    int G = 1;
-    while (G < 32 && 4LL * G * 2 <= avg) G *= 2;  // about four entries per lane
-    return G;
-}
-
+// Warp tiles: consecutive rows, at most kTileRows rows and kTileCap
+// entries; a row longer than kTileCap becomes kChunk-entry chunks.
 inline void build_tile_plan(const std::vector<int> &rp, TilePlan &p)
 {
     p = TilePlan();
@@ -246,7 +354,7 @@ inline void build_tile_plan(const std::vector<int> &rp, TilePlan &p)
     int r = 0;
     while (r < nrow) {
         const int len = rp[r + 1] - rp[r];
-        if (len > kLongRow) {
+        if (len > kTileCap) {
             p.long_rows.push_back(make_int2(r, (int)p.chunks.size()));
             for (int k = rp[r]; k < rp[r + 1]; k += kChunk) {
                 const int k1 = k + kChunk < rp[r + 1] ? k + kChunk : rp[r + 1];
@@ -255,14 +363,14 @@ inline void build_tile_plan(const std::vector<int> &rp, TilePlan &p)
             ++r;
             continue;
         }
-        if (len >= kSoloRow) {
-            p.tiles.push_back(make_int4(r, r + 1, 32, 0));
-            ++r;
-            continue;
+        int r1 = r, nnz = 0;
+        while (r1 < nrow && r1 - r < kTileRows) {
+            const int l = rp[r1 + 1] - rp[r1];
+            if (l > kTileCap || (nnz + l > kTileCap && r1 > r)) break;
+            nnz += l;
+            ++r1;
         }
-        int r1 = r;
-        while (r1 < nrow && r1 - r < 32 && rp[r1 + 1] - rp[r1] < kSoloRow) ++r1;
-        p.tiles.push_back(make_int4(r, r1, lane_group_for(rp[r1] - rp[r], r1 - r), 0));
+        p.tiles.push_back(make_int4(r, r1, nnz, 0));
         r = r1;
     }
 }

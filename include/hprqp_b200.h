@@ -16,11 +16,12 @@
 extern "C" {
 #endif
 
-/* y = M x with the engine's row-block SpMV kernel (the product inside every
+/* y = M x with the engine's tiled SpMV kernel (the product inside every
  * HPR step; the reference runs cuSPARSE CSR ALG2 or a thread-per-row dot,
- * src/gpu/spmv.cu:25-39, 511-659).  Host arrays in, host array out; the
- * kernel is replayed `reps` times (>= 1) and, when ms_per_spmv is non-NULL,
- * the mean device time of one product (CUDA events) is returned there.
+ * src/gpu/spmv.cu:25-39, 511-659).  Host arrays in, host array out; after
+ * one untimed launch the kernel is replayed `reps` times (>= 1) and, when
+ * ms_per_spmv is non-NULL, the mean device time of one product (CUDA
+ * events) is returned there.
  * A matrix whose stream is smaller than 256 MiB is evicted from L2 (a
  * 256 MiB buffer write) before every timed product, so each product reads it
  * from HBM; larger matrices do not fit in L2 and are timed back to back. */

@@ -5,6 +5,9 @@
 * ``_ref/libhprqp_ref_cpu.so``: the reference's own CPU backend compiled from
   its sources by ``make -C oracle ref`` (only possible where the reference
   sources exist; the built library travels with the repository snapshot).
+* ``_ref/libhprqp_ref_gpu.so``: the reference's own CUDA backend
+  (cuSPARSE/cuBLAS), ``make -C oracle ref-gpu``; called through its C API
+  (``solve_gpu``) with polishing and the Gram path off.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline legs use
 this module.
@@ -22,6 +25,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "lib" / "liboracle.so"
 REF_CPU_LIB = HERE / "_ref" / "libhprqp_ref_cpu.so"
+REF_GPU_LIB = HERE / "_ref" / "libhprqp_ref_gpu.so"
 
 MODE_GPU_REF = 0
 MODE_CPU_REF = 1
@@ -363,3 +367,130 @@ def ref_solve(inst, stoptol=1e-8, max_iter=2147483647, use_scaling=True, check_i
     L.hprqp_params_destroy(params)
     L.hprqp_model_destroy(model)
     return out
+
+
+# --------------------------------------------------------------------------
+# the reference's own GPU library (oracle/_ref), through its C API
+# --------------------------------------------------------------------------
+# Struct layouts of the reference's include/shared/types.h:10-214 (an ABI,
+# so they must match field for field).
+
+class _RefCSR(ctypes.Structure):
+    _fields_ = [("nrow", ctypes.c_size_t), ("ncol", ctypes.c_size_t), ("nnz", ctypes.c_size_t),
+                ("row_ptr", c_size_p), ("col_ind", c_size_p), ("values", c_double_p), ("owns_data", ctypes.c_int)]
+
+
+class _RefModel(ctypes.Structure):
+    _fields_ = [("Q", _RefCSR), ("A", _RefCSR), ("AT", _RefCSR), ("c", c_double_p), ("AL", c_double_p),
+                ("AU", c_double_p), ("l", c_double_p), ("u", c_double_p), ("obj_constant", ctypes.c_double),
+                ("owns_data", ctypes.c_int), ("num_var_cones", ctypes.c_size_t), ("var_cone_offsets", c_size_p),
+                ("num_row_cones", ctypes.c_size_t), ("row_cone_offsets", c_size_p), ("soc_rhs", c_double_p)]
+
+
+class _RefParams(ctypes.Structure):
+    _fields_ = [("stoptol", ctypes.c_double), ("max_iter", ctypes.c_size_t), ("use_gpu", ctypes.c_int),
+                ("device_number", ctypes.c_int), ("time_limit", ctypes.c_double),
+                ("check_iter", ctypes.c_size_t), ("print_frequency", ctypes.c_int),
+                ("use_scaling", ctypes.c_int), ("verbose", ctypes.c_int), ("spmv_mode_q", ctypes.c_int),
+                ("spmv_mode_a", ctypes.c_int), ("gram_mode", ctypes.c_int), ("polishing", ctypes.c_int),
+                ("polish_python", ctypes.c_char_p), ("polish_worker", ctypes.c_char_p),
+                ("polish_directory", ctypes.c_char_p), ("polish_keep_files", ctypes.c_int),
+                ("polish_max_attempts", ctypes.c_size_t), ("polish_episode_seconds", ctypes.c_double),
+                ("polish_total_seconds", ctypes.c_double), ("polish_memory_bytes", ctypes.c_size_t)]
+
+
+class _RefResults(ctypes.Structure):
+    _fields_ = [("iter", ctypes.c_size_t), ("iter_4", ctypes.c_size_t), ("iter_6", ctypes.c_size_t),
+                ("time", ctypes.c_double), ("time_4", ctypes.c_double), ("time_6", ctypes.c_double),
+                ("primal_obj", ctypes.c_double), ("residuals", ctypes.c_double), ("gap", ctypes.c_double),
+                ("status", ctypes.c_int), ("x", c_double_p), ("y", c_double_p), ("z", c_double_p),
+                ("w", c_double_p), ("polish_attempts", ctypes.c_size_t), ("polish_accepted", ctypes.c_int),
+                ("gram_active", ctypes.c_int), ("total_time", ctypes.c_double)]
+
+
+_ref_gpu: Optional[ctypes.CDLL] = None
+
+
+def ref_gpu_available() -> bool:
+    return REF_GPU_LIB.exists()
+
+
+def ref_gpu_lib() -> ctypes.CDLL:
+    global _ref_gpu
+    if _ref_gpu is None:
+        L = ctypes.CDLL(str(REF_GPU_LIB))
+        L.model_init.argtypes = [ctypes.POINTER(_RefModel)]
+        L.model_free.argtypes = [ctypes.POINTER(_RefModel)]
+        L.build_from_QAbc.argtypes = [ctypes.POINTER(_RefCSR), ctypes.POINTER(_RefCSR)] + [c_double_p] * 5 + \
+            [ctypes.c_double, ctypes.POINTER(_RefModel)]
+        L.params_set_defaults.argtypes = [ctypes.POINTER(_RefParams)]
+        L.results_init.argtypes = [ctypes.POINTER(_RefResults)]
+        L.results_free.argtypes = [ctypes.POINTER(_RefResults)]
+        L.solve_gpu.argtypes = [ctypes.POINTER(_RefModel), ctypes.POINTER(_RefParams), ctypes.POINTER(_RefResults)]
+        L.gpu_backend_available.restype = ctypes.c_int
+        _ref_gpu = L
+    return _ref_gpu
+
+
+class RefGpuModel:
+    """A model built by the reference's own ``build_from_QAbc`` inside the
+    reference GPU library; ``solve`` runs its ``solve_gpu`` (polishing 0,
+    Gram off: the reference with ``--polishing 0 --gram off``)."""
+
+    def __init__(self, inst):
+        L = ref_gpu_lib()
+        self._keep = []
+
+        def csr(nrow, ncol, m):
+            ip, pp = _sz(np.asarray(m.indptr))
+            ii, pi = _sz(np.asarray(m.indices) if m.nnz else np.zeros(1))
+            dd, pd = _db(np.asarray(m.data) if m.nnz else np.zeros(1))
+            self._keep += [ip, ii, dd]
+            return _RefCSR(nrow, ncol, m.nnz, pp, pi, pd, 0)
+
+        def db(a):
+            arr, p = _db(a if len(a) else np.zeros(1))
+            self._keep.append(arr)
+            return p
+
+        Q = csr(inst.n, inst.n, inst.Q)
+        A = csr(inst.m, inst.n, inst.A)
+        self.model = _RefModel()
+        L.model_init(ctypes.byref(self.model))
+        st = L.build_from_QAbc(ctypes.byref(Q), ctypes.byref(A), db(inst.c), db(inst.AL), db(inst.AU),
+                               db(inst.l), db(inst.u), float(inst.obj_constant), ctypes.byref(self.model))
+        if st != 0:
+            raise ValueError(f"reference build_from_QAbc failed: {st}")
+        self.n = int(self.model.Q.ncol)
+        self.m = int(self.model.A.nrow)
+
+    def solve(self, stoptol=1e-6, max_iter=2147483647, time_limit=3600.0, device=0):
+        L = ref_gpu_lib()
+        p = _RefParams()
+        L.params_set_defaults(ctypes.byref(p))
+        p.stoptol = stoptol
+        p.max_iter = max_iter
+        p.time_limit = time_limit
+        p.use_gpu = 1
+        p.device_number = device
+        p.verbose = 0
+        p.polishing = 0
+        p.gram_mode = 0
+        r = _RefResults()
+        L.results_init(ctypes.byref(r))
+        st = L.solve_gpu(ctypes.byref(self.model), ctypes.byref(p), ctypes.byref(r))
+
+        def vec(ptr, k):
+            return np.ctypeslib.as_array(ptr, shape=(k,)).copy() if (ptr and k) else np.zeros(0)
+
+        out = dict(ret=st, status=r.status, iter=int(r.iter), primal_obj=r.primal_obj, residuals=r.residuals,
+                   gap=r.gap, time=r.time, x=vec(r.x, self.n), y=vec(r.y, self.m), z=vec(r.z, self.n),
+                   w=vec(r.w, self.n))
+        L.results_free(ctypes.byref(r))
+        return out
+
+    def __del__(self):
+        try:
+            ref_gpu_lib().model_free(ctypes.byref(self.model))
+        except Exception:
+            pass
