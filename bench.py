@@ -184,6 +184,47 @@ def spmv_leg(peak_gbs: float, reps: int = 10):
     return out
 
 
+def large_qp_leg(peak_gbs: float, iters: int = 3000):
+    """Plain solve_gpu on the large power-law QP (n=1e6, m=5e5, nnz(A)~1e7,
+    nnz(Q)~3.2e7, stoptol 1e-8) for a fixed iteration budget (it does not
+    reach 1e-8 within minutes, neither here nor with the reference's GPU
+    build): HPR iterations/s of the solve loop and the HBM roofline of its
+    algorithmic bytes (B_iter per iteration)."""
+    import hprqp
+    from hprqp import instances
+
+    inst = instances.config1()
+    model = hprqp.build_from_instance(inst)
+    params = hprqp.Parameters(verbose=False, stoptol=1e-8, max_iter=iters)
+    t0 = time.perf_counter()
+    r = hprqp.optimize(model, params, as_numpy=True)
+    wall = time.perf_counter() - t0
+    ips = r.iter / r.time
+    gbs = bytes_per_iter(inst) * ips / 1e9
+    return {"workload": "n=1e6 m=5e5 power-law QP, stoptol 1e-8", "iterations": int(r.iter),
+            "loop_s": round(r.time, 4), "call_s": round(wall, 3), "iters_per_s": round(ips, 1),
+            "bytes_per_iter": bytes_per_iter(inst), "GB/s": round(gbs, 1), "frac": round(gbs / peak_gbs, 4),
+            "kkt": float(r.residual), "status": r.status}
+
+
+def portfolio_leg():
+    """Plain solve_gpu on the factor-structured portfolio QP (n=200,200,
+    200 dense factor rows, diagonal Q) to 1e-6."""
+    import hprqp
+    from hprqp import instances
+
+    inst = instances.config2()
+    model = hprqp.build_from_instance(inst)
+    params = hprqp.Parameters(verbose=False, stoptol=1e-6)
+    hprqp.optimize(model, hprqp.Parameters(verbose=False, stoptol=1e-6, max_iter=10), as_numpy=True)
+    t0 = time.perf_counter()
+    r = hprqp.optimize(model, params, as_numpy=True)
+    wall = time.perf_counter() - t0
+    return {"workload": "portfolio n=200,200 (k=200 factors, 500 sectors), stoptol 1e-6", "status": r.status,
+            "iterations": int(r.iter), "loop_s": round(r.time, 4), "call_s": round(wall, 3),
+            "iters_per_s": round(r.iter / r.time, 1), "objective": r.objective, "kkt": float(r.residual)}
+
+
 def adjoint_leg(device: int, count: int = 256, reps: int = 3):
     """Differentiation workload: 256 QPs (n=500, m=300, 150 equality rows),
     forward solve to 1e-8, loss L = sum g.x* with g ~ N(0,1) per instance,
@@ -278,8 +319,10 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--no-spmv", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--only", choices=["spmv", "batch", "adjoint"], default=None,
-                    help="profiling sub-runs: only the large-QP SpMV leg, the batched solve, or the adjoint")
+    ap.add_argument("--no-plain-large", action="store_true")
+    ap.add_argument("--only", choices=["spmv", "batch", "adjoint", "large", "portfolio"], default=None,
+                    help="sub-runs: only the large-QP SpMV leg, the batched solve, the adjoint, the large-QP "
+                         "plain solve or the portfolio plain solve")
     ap.add_argument("--spmv-reps", type=int, default=10)
     args = ap.parse_args()
 
@@ -332,6 +375,12 @@ def main():
         return
     if args.only == "adjoint":
         print(json.dumps({"adjoint": adjoint_leg(local_rank)}), flush=True)
+        return
+    if args.only == "large":
+        print(json.dumps({"large_qp": large_qp_leg(peak)}), flush=True)
+        return
+    if args.only == "portfolio":
+        print(json.dumps({"portfolio": portfolio_leg()}), flush=True)
         return
     insts = batch_instances(args.batch, 100000 * rank)
     packed = hb.pack(insts)
@@ -420,6 +469,9 @@ def main():
             line["spmv"] = spmv_leg(peak)
         if not args.no_adjoint:
             line["adjoint"] = adjoint_leg(local_rank)
+        if not args.no_plain_large:
+            line["large_qp"] = large_qp_leg(peak)
+            line["portfolio"] = portfolio_leg()
         ids = list(range(min(args.cpu_sample, args.batch)))
         rate, kind, cdt, _ = cpu_reference_rate(ids, cores)
         line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind,
