@@ -184,12 +184,13 @@ def spmv_leg(peak_gbs: float, reps: int = 10):
     return out
 
 
-def large_qp_leg(peak_gbs: float, iters: int = 3000):
+def large_qp_leg(peak_gbs: float, iters: int = 3000, minres_iters: int = 2000):
     """Plain solve_gpu on the large power-law QP (n=1e6, m=5e5, nnz(A)~1e7,
     nnz(Q)~3.2e7, stoptol 1e-8) for a fixed iteration budget (it does not
     reach 1e-8 within minutes, neither here nor with the reference's GPU
     build): HPR iterations/s of the solve loop and the HBM roofline of its
-    algorithmic bytes (B_iter per iteration)."""
+    algorithmic bytes (B_iter per iteration); then the single-instance
+    adjoint (hprqp_diff.h) on that iterate."""
     import hprqp
     from hprqp import instances
 
@@ -197,14 +198,24 @@ def large_qp_leg(peak_gbs: float, iters: int = 3000):
     model = hprqp.build_from_instance(inst)
     params = hprqp.Parameters(verbose=False, stoptol=1e-8, max_iter=iters)
     t0 = time.perf_counter()
-    r = hprqp.optimize(model, params, as_numpy=True)
+    r, state = hprqp.solve_for_backward(model, params)
     wall = time.perf_counter() - t0
     ips = r.iter / r.time
     gbs = bytes_per_iter(inst) * ips / 1e9
-    return {"workload": "n=1e6 m=5e5 power-law QP, stoptol 1e-8", "iterations": int(r.iter),
-            "loop_s": round(r.time, 4), "call_s": round(wall, 3), "iters_per_s": round(ips, 1),
-            "bytes_per_iter": bytes_per_iter(inst), "GB/s": round(gbs, 1), "frac": round(gbs / peak_gbs, 4),
-            "kkt": float(r.residual), "status": r.status}
+    out = {"workload": "n=1e6 m=5e5 power-law QP, stoptol 1e-8", "iterations": int(r.iter),
+           "loop_s": round(r.time, 4), "call_s": round(wall, 3), "iters_per_s": round(ips, 1),
+           "bytes_per_iter": bytes_per_iter(inst), "GB/s": round(gbs, 1), "frac": round(gbs / peak_gbs, 4),
+           "kkt": float(r.residual), "status": r.status}
+    if state is not None:
+        # single-instance backward at this size: L = g.x*, g ~ N(0,1), on the
+        # active set of the iterate above, a fixed MINRES budget
+        g = state.backward(np.random.default_rng(1).standard_normal(r.x.shape[0]), tol=1e-10,
+                           max_iter=minres_iters)
+        state.close()
+        out["backward"] = {"minres_iters": g["minres_iters"], "relres": g["minres_relres"],
+                           "seconds": round(g["backward_seconds"], 3),
+                           "ms_per_minres_iter": round(1e3 * g["backward_seconds"] / max(g["minres_iters"], 1), 4)}
+    return out
 
 
 def portfolio_leg():

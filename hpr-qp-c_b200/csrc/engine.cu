@@ -1618,6 +1618,219 @@ HPRQPStatus engine_copy_output(Engine *e, double *x, double *w, double *z, doubl
     return HPRQP_STATUS_OK;
 }
 
+// ---- implicit-differentiation adjoint on the device-wide kernels ------------
+// MINRES on P Ks P with Ks = [[Q_s, A_s'], [A_s, 0]] (the scaled matrices of
+// the finished solve), P the 0/1 active-set mask (z_bar == 0 on variables,
+// y_bar != 0 on rows).  Vectors are [n-part | m-part] of length n + m.
+struct EpiAdjInit : EpiBase<1> {  // v <- D^-1 P [gx; -gy], acc += v^2  (len n + m)
+    int n;
+    const double *zb, *yb, *cn, *rn, *gx, *gy;
+    double *v;
+    __device__ void row(int i, double, Acc<1> &a) const
+    {
+        double t;
+        if (i < n) t = zb[i] == 0.0 ? gx[i] / cn[i] : 0.0;
+        else t = (gy && yb[i - n] != 0.0) ? -gy[i - n] / rn[i - n] : 0.0;
+        v[i] = t;
+        a.v[0] += t * t;
+    }
+};
+struct EpiAdjScale : EpiBase<0> {
+    double *v;
+    double s;
+    __device__ void row(int i, double, Acc<0> &) const { v[i] *= s; }
+};
+struct EpiAdjM : EpiBase<1> {  // vn_m = P_m (A_s v_n), acc += v_m . vn_m
+    const double *yb, *vm;
+    double *vnm;
+    __device__ void row(int r, double a, Acc<1> &acc) const
+    {
+        const double t = yb[r] != 0.0 ? a : 0.0;
+        vnm[r] = t;
+        acc.v[0] += vm[r] * t;
+    }
+};
+struct EpiAdjN : EpiBase<1> {  // vn_n = P_n (Q_s v_n + A_s' v_m), acc += v_n . vn_n
+    const double *zb, *tmp, *vn;
+    double *vnn;
+    __device__ void row(int i, double s, Acc<1> &acc) const
+    {
+        const double t = zb[i] == 0.0 ? (tmp ? tmp[i] + s : s) : 0.0;
+        vnn[i] = t;
+        acc.v[0] += vn[i] * t;
+    }
+};
+struct EpiAdjLanczos : EpiBase<1> {  // vn <- vn - alpha v - beta vo, acc += vn^2  (len n + m)
+    double *vn;
+    const double *v, *vo;
+    double alpha, beta;
+    __device__ void row(int i, double, Acc<1> &a) const
+    {
+        const double t = vn[i] - alpha * v[i] - beta * vo[i];
+        vn[i] = t;
+        a.v[0] += t * t;
+    }
+};
+struct EpiAdjStep : EpiBase<0> {  // direction update, solution update, Lanczos normalisation
+    const double *v, *wo, *w;
+    double *wn, *sol, *vn;
+    double r2, r3, inv_r1, step, inv_b;
+    __device__ void row(int i, double, Acc<0> &) const
+    {
+        const double d = (v[i] - r3 * wo[i] - r2 * w[i]) * inv_r1;
+        wn[i] = d;
+        sol[i] += step * d;
+        vn[i] *= inv_b;
+    }
+};
+struct EpiAdjOut : EpiBase<0> {  // lambda = sol_n / col_norm, mu = sol_m / row_norm
+    int n;
+    const double *sol, *cn, *rn;
+    double *out;
+    __device__ void row(int i, double, Acc<0> &) const { out[i] = i < n ? sol[i] / cn[i] : sol[i] / rn[i - n]; }
+};
+
+HPRQPStatus engine_adjoint(Engine *e, const double *gx, const double *gy, double tol, long long maxit,
+                           double *lam, double *mu, long long *iters, double *relres)
+{
+    DState &S = e->S;
+    const int n = S.n, m = S.m, len = n + m;
+    HPR_CK(cudaSetDevice(e->device));
+    if (len == 0) {
+        *iters = 0;
+        *relres = 0.0;
+        return HPRQP_STATUS_OK;
+    }
+    double *blk = nullptr;
+    HPRQPStatus st = dalloc(e, &blk, (size_t)9 * len + 2);
+    if (st) return st;
+    double *vb[3] = {blk, blk + len, blk + 2 * (size_t)len};
+    double *wb[3] = {blk + 3 * (size_t)len, blk + 4 * (size_t)len, blk + 5 * (size_t)len};
+    double *sol = blk + 6 * (size_t)len, *tmp = blk + 7 * (size_t)len, *g = blk + 8 * (size_t)len;
+    HPR_CK(cudaMemsetAsync(blk, 0, (size_t)9 * len * sizeof(double), e->stream));
+    if (n) HPR_CK(cudaMemcpyAsync(g, gx, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    if (m && gy) HPR_CK(cudaMemcpyAsync(g + n, gy, m * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    double *vo = vb[0], *v = vb[1], *vn = vb[2], *wo = wb[0], *w = wb[1], *wn = wb[2];
+    // right-hand side and beta0
+    EpiAdjInit ini;
+    ini.n = n;
+    ini.zb = S.z_bar;
+    ini.yb = S.y_bar;
+    ini.cn = S.col_norm;
+    ini.rn = S.row_norm;
+    ini.gx = g;
+    ini.gy = gy ? g + n : nullptr;
+    ini.v = v;
+    int gsz = launch_ew(e, len, ini, 0);
+    FinSpec f0 = spec_of<EpiAdjInit>(gsz, 0, 0);
+    if ((st = finalize(e, &f0, 1, true))) return st;
+    const double beta0 = sqrt(e->hout->v[0]);
+    double beta = beta0, eta = beta0, c_old = 1.0, c = 1.0, s_old = 0.0, s = 0.0;
+    long long it = 0;
+    if (beta0 > 0.0) {
+        EpiAdjScale sc;
+        sc.v = v;
+        sc.s = 1.0 / beta0;
+        launch_ew(e, len, sc);
+        const size_t pa = 0, pat = (size_t)std::max(S.A.npart(), 1);
+        for (it = 0; it < maxit; ++it) {
+            // vn = P Ks P v, alpha = v . vn
+            FinSpec fa[2];
+            int nf = 0;
+            if (m > 0) {
+                EpiStore q;
+                q.out = tmp;
+                launch_rb(e, S.Q, v, q);
+                EpiAdjM am;
+                am.yb = S.y_bar;
+                am.vm = v + n;
+                am.vnm = vn + n;
+                launch_rb_at(e, S.A, v, am, pa);
+                fa[nf++] = spec_of<EpiAdjM>(S.A.npart(), 0, pa);
+                EpiAdjN an;
+                an.zb = S.z_bar;
+                an.tmp = tmp;
+                an.vn = v;
+                an.vnn = vn;
+                launch_rb_at(e, S.AT, v + n, an, pat);
+                fa[nf++] = spec_of<EpiAdjN>(S.AT.npart(), 1, pat);
+            } else {
+                EpiAdjN an;
+                an.zb = S.z_bar;
+                an.tmp = nullptr;
+                an.vn = v;
+                an.vnn = vn;
+                launch_rb_at(e, S.Q, v, an, pa);
+                fa[nf++] = spec_of<EpiAdjN>(S.Q.npart(), 0, pa);
+            }
+            if ((st = finalize(e, fa, nf, true))) return st;
+            const double alpha = e->hout->v[0] + (nf > 1 ? e->hout->v[1] : 0.0);
+            EpiAdjLanczos lz;
+            lz.vn = vn;
+            lz.v = v;
+            lz.vo = vo;
+            lz.alpha = alpha;
+            lz.beta = beta;
+            gsz = launch_ew(e, len, lz, 0);
+            FinSpec fb = spec_of<EpiAdjLanczos>(gsz, 0, 0);
+            if ((st = finalize(e, &fb, 1, true))) return st;
+            const double beta_new = sqrt(e->hout->v[0]);
+            // Givens QR of the new tridiagonal column (Paige-Saunders)
+            const double r1h = c * alpha - c_old * s * beta;
+            const double r1 = sqrt(r1h * r1h + beta_new * beta_new);
+            const double r2 = s * alpha + c_old * c * beta;
+            const double r3 = s_old * beta;
+            const double c_new = r1 > 0.0 ? r1h / r1 : 1.0;
+            const double s_new = r1 > 0.0 ? beta_new / r1 : 0.0;
+            EpiAdjStep up;
+            up.v = v;
+            up.wo = wo;
+            up.w = w;
+            up.wn = wn;
+            up.sol = sol;
+            up.vn = vn;
+            up.r2 = r2;
+            up.r3 = r3;
+            up.inv_r1 = r1 > 0.0 ? 1.0 / r1 : 0.0;
+            up.step = c_new * eta;
+            up.inv_b = beta_new > 0.0 ? 1.0 / beta_new : 0.0;
+            launch_ew(e, len, up);
+            eta = -s_new * eta;
+            double *t0 = vo;
+            vo = v;
+            v = vn;
+            vn = t0;
+            t0 = wo;
+            wo = w;
+            w = wn;
+            wn = t0;
+            beta = beta_new;
+            c_old = c;
+            c = c_new;
+            s_old = s;
+            s = s_new;
+            if (fabs(eta) <= tol * beta0 || beta_new == 0.0) {
+                ++it;
+                break;
+            }
+        }
+    }
+    EpiAdjOut o;
+    o.n = n;
+    o.sol = sol;
+    o.cn = S.col_norm;
+    o.rn = S.row_norm;
+    o.out = tmp;  // reuse: n + m entries
+    launch_ew(e, len, o);
+    if (n) HPR_CK(cudaMemcpyAsync(lam, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    if (m) HPR_CK(cudaMemcpyAsync(mu, tmp + n, m * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    HPR_CK(cudaStreamSynchronize(e->stream));
+    HPR_CK(cudaGetLastError());
+    *iters = it;
+    *relres = beta0 > 0.0 ? fabs(eta) / beta0 : 0.0;
+    return HPRQP_STATUS_OK;
+}
+
 HPRQPStatus engine_dump_scaling(Engine *e, ScaleDump *d)
 {
     DState &S = e->S;

@@ -45,6 +45,18 @@ struct ScaleDump {
 };
 HPRQPStatus engine_dump_scaling(Engine *e, ScaleDump *d);
 
+// Implicit-differentiation adjoint of the finished solve held by e: MINRES
+// on the scaled active-set KKT operator (variables with z_bar == 0, rows with
+// y_bar != 0).  gx (n) and gy (m, may be NULL) are host arrays in the model's
+// space; lam (n) and mu (m) receive the adjoint solution in original space.
+HPRQPStatus engine_adjoint(Engine *e, const double *gx, const double *gy, double tol, long long maxit,
+                           double *lam, double *mu, long long *iters, double *relres);
+
+// solve_gpu that hands its engine (scaled problem + final iterate) to the
+// caller instead of destroying it (*keep is set only on a terminal status).
+HPRQPStatus solve_gpu_keep(const HPRQPModel *model, const HPRQPParams *params, HPRQPResults *results,
+                           Engine **keep);
+
 // Kernel launch counter (process-wide, all engine kernels).
 uint64_t launch_count();
 void count_launch(uint64_t k = 1);

@@ -219,8 +219,14 @@ int gpu_backend_available(void)
     return 0;
 }
 
-HPRQPStatus solve_gpu(const HPRQPModel *model, const HPRQPParams *params, HPRQPResults *results)
+}  // extern "C"
+
+// solve_gpu, optionally handing the engine (scaled problem and final
+// iterate) to the caller for the adjoint instead of destroying it.
+HPRQPStatus hpr::solve_gpu_keep(const HPRQPModel *model, const HPRQPParams *params, HPRQPResults *results,
+                                hpr::Engine **keep)
 {
+    if (keep) *keep = nullptr;
     const double t_begin = now_s();
     if (!model || !params || !results) return HPRQP_STATUS_INVALID_ARGUMENT;
     if (params->gram_mode < HPRQP_GRAM_OFF || params->gram_mode > HPRQP_GRAM_REQUEST)
@@ -376,9 +382,19 @@ HPRQPStatus solve_gpu(const HPRQPModel *model, const HPRQPParams *params, HPRQPR
         ret = final_status;
     }
 done:
-    hpr::engine_destroy(eng);
+    if (keep && (ret == HPRQP_STATUS_OPTIMAL || ret == HPRQP_STATUS_MAX_ITER || ret == HPRQP_STATUS_TIME_LIMIT))
+        *keep = eng;
+    else
+        hpr::engine_destroy(eng);
     results->total_time = now_s() - t_begin;
     return ret;
+}
+
+extern "C" {
+
+HPRQPStatus solve_gpu(const HPRQPModel *model, const HPRQPParams *params, HPRQPResults *results)
+{
+    return hpr::solve_gpu_keep(model, params, results, nullptr);
 }
 
 HPRQPStatus solve(const HPRQPModel *model, const HPRQPParams *params, HPRQPResults *results)

@@ -109,6 +109,13 @@ class _Library:
     @staticmethod
     def _configure(lib: ctypes.CDLL) -> None:
         vp = ctypes.c_void_p
+        lib.hprqp_solve_for_backward.argtypes = [ctypes.c_void_p] * 3 + [ctypes.POINTER(ctypes.c_void_p)]
+        lib.hprqp_solve_for_backward.restype = ctypes.c_int
+        lib.hprqp_backward.argtypes = [ctypes.c_void_p, c_double_p, c_double_p, ctypes.c_double, ctypes.c_longlong,
+                                       ctypes.c_void_p]
+        lib.hprqp_backward.restype = ctypes.c_int
+        lib.hprqp_solve_state_destroy.argtypes = [ctypes.c_void_p]
+        lib.hprqp_solve_state_destroy.restype = None
         lib.hprqp_status_name.argtypes = [ctypes.c_int]
         lib.hprqp_status_name.restype = ctypes.c_char_p
         lib.hprqp_gpu_backend_available.restype = ctypes.c_int
@@ -420,6 +427,91 @@ def optimize(model: Model, params: Optional[Parameters] = None, as_numpy: bool =
         lib.hprqp_results_destroy(results_handle)
 
 
+class _ResultsStruct(ctypes.Structure):
+    _fields_ = [("iter", ctypes.c_size_t), ("iter_4", ctypes.c_size_t), ("iter_6", ctypes.c_size_t),
+                ("time", ctypes.c_double), ("time_4", ctypes.c_double), ("time_6", ctypes.c_double),
+                ("primal_obj", ctypes.c_double), ("residuals", ctypes.c_double), ("gap", ctypes.c_double),
+                ("status", ctypes.c_int), ("x", c_double_p), ("y", c_double_p), ("z", c_double_p),
+                ("w", c_double_p), ("polish_attempts", ctypes.c_size_t), ("polish_accepted", ctypes.c_int),
+                ("gram_active", ctypes.c_int), ("total_time", ctypes.c_double)]
+
+
+class _GradientsStruct(ctypes.Structure):
+    _fields_ = [(k, c_double_p) for k in ("dc", "dl", "du", "dAL", "dAU", "dQ_values", "dA_values", "lam", "mu")] + \
+               [("minres_iters", ctypes.c_longlong), ("minres_relres", ctypes.c_double),
+                ("backward_seconds", ctypes.c_double)]
+
+
+class SolveState:
+    """Device state of a finished solve, kept for :meth:`backward`
+    (hprqp_diff.h).  Gradients are in the space of the model (its symmetrised
+    Q, the rows of A kept by preprocessing), like the solution."""
+
+    def __init__(self, model: "Model", handle: ctypes.c_void_p):
+        self._model = model  # the state reads the model: keep it alive
+        self._handle = handle
+        ms = model._struct()
+        self.n, self.m = int(ms.Q.ncol), int(ms.A.nrow)
+        self.q_nnz, self.a_nnz = int(ms.Q.nnz), int(ms.A.nnz)
+
+    def backward(self, grad_x, grad_y=None, tol: float = 1e-12, max_iter: int = 0) -> dict:
+        gx = np.ascontiguousarray(np.broadcast_to(np.asarray(grad_x, np.float64), (self.n,)))
+        gy = None if grad_y is None else np.ascontiguousarray(
+            np.broadcast_to(np.asarray(grad_y, np.float64), (self.m,)))
+        out = {k: np.zeros(max(v, 1)) for k, v in (("dc", self.n), ("dl", self.n), ("du", self.n), ("dAL", self.m),
+                                                   ("dAU", self.m), ("dQ_values", self.q_nnz),
+                                                   ("dA_values", self.a_nnz), ("lam", self.n), ("mu", self.m))}
+        g = _GradientsStruct(**{k: v.ctypes.data_as(c_double_p) for k, v in out.items()})
+        gxp = (gx if self.n else np.zeros(1)).ctypes.data_as(c_double_p)
+        gyp = None if gy is None else (gy if self.m else np.zeros(1)).ctypes.data_as(c_double_p)
+        _raise_for_status(_lib().hprqp_backward(self._handle, gxp, gyp, float(tol), int(max_iter), ctypes.byref(g)),
+                          "hprqp_backward")
+        sizes = {"dc": self.n, "dl": self.n, "du": self.n, "dAL": self.m, "dAU": self.m, "dQ_values": self.q_nnz,
+                 "dA_values": self.a_nnz, "lam": self.n, "mu": self.m}
+        res = {k: out[k][:sizes[k]] for k in out}
+        res.update(minres_iters=int(g.minres_iters), minres_relres=float(g.minres_relres),
+                   backward_seconds=float(g.backward_seconds))
+        return res
+
+    def close(self) -> None:
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value and _Library._instance is not None:
+            _Library._instance.hprqp_solve_state_destroy(h)
+            h.value = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_for_backward(model: Model, params: Optional[Parameters] = None):
+    """``optimize`` that keeps the solve's device state for the adjoint:
+    returns ``(Result, SolveState or None)`` (include/hprqp_diff.h)."""
+    if params is None:
+        params = Parameters()
+    lib = _lib()
+    results_handle = ctypes.c_void_p()
+    _raise_for_status(lib.hprqp_results_create(ctypes.byref(results_handle)), "hprqp_results_create")
+    state = ctypes.c_void_p()
+    try:
+        code = int(lib.hprqp_solve_for_backward(model._handle, params._handle, results_handle, ctypes.byref(state)))
+        r = ctypes.cast(results_handle, ctypes.POINTER(_ResultsStruct)).contents
+        n, m = model.num_variables, model.num_constraints
+
+        def vec(ptr, k):
+            return np.ctypeslib.as_array(ptr, shape=(k,)).copy() if (ptr and k) else np.zeros(0)
+
+        res = Result(status_code=code, status=status_name(code), iter=int(r.iter), iter_4=int(r.iter_4),
+                     iter_6=int(r.iter_6), time=float(r.time), time_4=float(r.time_4), time_6=float(r.time_6),
+                     objective=float(r.primal_obj), residual=float(r.residuals), gap=float(r.gap),
+                     x=vec(r.x, n), y=vec(r.y, m), z=vec(r.z, n), w=vec(r.w, n))
+    finally:
+        lib.hprqp_results_destroy(results_handle)
+    return res, (SolveState(model, state) if state.value else None)
+
+
 def spmv(indptr, indices, data, ncol: int, x, reps: int = 1):
     """y = M x on the GPU with the engine's row-block kernel.
     Returns (y, mean_ms_per_product)."""
@@ -500,7 +592,7 @@ def __getattr__(name):
 
 
 __all__ = [
-    "QPFunction", "QPLayer", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
+    "QPFunction", "QPLayer", "SolveState", "solve_for_backward", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
     "STATUS_ALLOCATION_FAILED", "STATUS_CONTINUE", "STATUS_INVALID_ARGUMENT", "STATUS_MAX_ITER",
     "STATUS_NOT_IMPLEMENTED", "STATUS_OK", "STATUS_OPTIMAL", "STATUS_TIME_LIMIT", "build_from_mps",
     "build_from_QAbc", "build_from_qabc", "build_from_instance", "gpu_backend_available", "optimize",
