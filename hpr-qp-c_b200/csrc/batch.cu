@@ -45,27 +45,13 @@ namespace hpr {
 #endif
 constexpr int kBT = HPR_BATCH_THREADS;  // threads per CTA of the batch kernel
 constexpr int kBW = kBT / 32;
-#ifndef HPR_BATCH_WIN_U
-#define HPR_BATCH_WIN_U 4  // entries per lane per SpMV window
-#endif
-#ifndef HPR_BATCH_PREFETCH
-#define HPR_BATCH_PREFETCH 1  // issue the next window's loads before summing the current one
-#endif
-constexpr int kBU = HPR_BATCH_WIN_U;
-constexpr int kWin = 32 * kBU;              // entries per warp window of the CTA SpMV
-constexpr int kWinPad = kWin + kWin / 8;    // padded product slots per warp
-constexpr int kBTileRows = 32;              // rows per SpMV tile (one per lane)
-constexpr int kBTileCap = 512;              // entries per SpMV tile (a longer row is a tile of its own)
-// per warp: kWinPad product slots, kBTileRows row sums, kWin head-flag bytes
-constexpr size_t kScratchDoubles = (size_t)kBW * (kWinPad + kBTileRows + kWin / 8);
-constexpr size_t kScratchBytes = kScratchDoubles * sizeof(double);
+constexpr int kWin = 256;  // entries per warp window of the flat SpMV (8 per lane)
+constexpr size_t kScratchBytes = (size_t)kBW * kWin * sizeof(double);
 constexpr size_t kSmemLimit = 220 * 1024;  // dynamic shared memory of the batch kernel
 
 struct BInst {
     long long q_nz, a_nz, at_nz;  // first entry of the instance's matrices
     int q_rp, a_rp, at_rp;        // first row pointer
-    int q_t, a_t, at_t;           // first SpMV tile of each matrix
-    int q_nt, a_nt, at_nt;        // SpMV tiles of each matrix
     int var, row;                 // first variable / row in the packed vectors
     int n, m;
     double obj_constant;
@@ -77,7 +63,6 @@ struct BatchArgs {
     const int *order;
     int *counter;
     const int *q_rp, *q_ci, *a_rp, *a_ci, *at_rp, *at_ci;
-    const int2 *tiles;  // SpMV tiles {first row, end row}, local rows
     const double *q_v0, *a_v0, *at_v0, *c0, *l0, *u0, *AL0, *AU0;
     double *q_v, *a_v, *at_v;  // scaled copies
     double *ws;                // per-CTA workspace
@@ -127,8 +112,6 @@ struct LCsr {
     const int *rp;
     const int *ci;
     const double *v;
-    const int2 *tiles;  // consecutive rows, at most kBTileRows rows / kBTileCap entries each
-    int ntiles;
 };
 
 __device__ __forceinline__ double clampd(double v, double lo, double hi)
@@ -159,102 +142,48 @@ __device__ __forceinline__ void cta_allreduce(double (&v)[N], const int (&ops)[N
     for (int k = 0; k < N; ++k) v[k] = s_out[k];
 }
 
-// y = M x over the matrix's tiles (up to 32 rows and 512 entries each),
-// warp w taking tiles w, w + 32, ...; f(row, y_row) is called once per row by
-// the lane that owns it.  A warp streams its tile as flat windows of 32 x
-// kBU entries: kBU coalesced index/value loads per lane (the next window's issued before
-// the current one is summed), products staged in the warp's scratch, row sums
-// by a segmented scan (head flags at row starts, a carry between windows), so
-// no lane waits on another's row length.
-__device__ __forceinline__ int bwin_slot(int i) { return i + (i >> 3); }
-
+// y = M x over 32-row warp tiles; f(row, y_row) is called by the lane that
+// owns the row (coalesced over consecutive rows).  A warp reads its tile's
+// entries as one flat, coalesced stream: eight independent index/value loads
+// per lane per 256-entry window, products staged in the warp's scratch, then
+// lane i adds row i's products in order.
 template <class F>
 __device__ __forceinline__ void cta_spmv(const LCsr &M, const double *x, double *scratch, F &&f)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double *sv = scratch + warp * kWinPad;
-    double *rowsum = scratch + kBW * kWinPad + warp * kBTileRows;
-    unsigned char *sh = reinterpret_cast<unsigned char *>(scratch + kBW * (kWinPad + kBTileRows)) + warp * kWin;
-    for (int t = warp; t < M.ntiles; t += kBW) {
-        const int2 T = M.tiles[t];
-        const int r0 = T.x, nr = T.y - T.x;
-        const int k0 = HPR_BATCH_LD(M.rp + r0), k1 = HPR_BATCH_LD(M.rp + r0 + nr);
-        const int a = lane < nr ? HPR_BATCH_LD(M.rp + r0 + lane) : k1;
-        const int e = lane < nr ? HPR_BATCH_LD(M.rp + r0 + lane + 1) : k1;
-        rowsum[lane] = 0.0;  // empty rows keep 0
-        double carry = 0.0;
-        int c[kBU];
-        double v[kBU];
-#pragma unroll
-        for (int u = 0; u < kBU; ++u) {
-            const int k = k0 + u * 32 + lane;
-            c[u] = k < k1 ? HPR_BATCH_LD(M.ci + k) : 0;
-            v[u] = k < k1 ? HPR_BATCH_LD(M.v + k) : 0.0;
-        }
+    double *sc = scratch + warp * kWin;
+    const int ntiles = (M.nrow + 31) >> 5;
+    for (int t = warp; t < ntiles; t += kBW) {
+        const int r0 = t << 5;
+        const int nr = min(32, M.nrow - r0);
+        const int k0 = M.rp[r0], k1 = M.rp[r0 + nr];
+        const int a = lane < nr ? M.rp[r0 + lane] : k1;
+        const int e = lane < nr ? M.rp[r0 + lane + 1] : k1;
+        double mine = 0.0;
         for (int base = k0; base < k1; base += kWin) {
-            const int nb = base + kWin;
-            double p[kBU];
+            int c[8];
+            double v[8];
 #pragma unroll
-            for (int u = 0; u < kBU; ++u) p[u] = v[u] * x[c[u]];
-            if (HPR_BATCH_PREFETCH || nb < k1) {
-#pragma unroll
-                for (int u = 0; u < kBU; ++u) {
-                    const int k = nb + u * 32 + lane;
-                    c[u] = k < k1 ? HPR_BATCH_LD(M.ci + k) : 0;
-                    v[u] = k < k1 ? HPR_BATCH_LD(M.v + k) : 0.0;
-                }
+            for (int u = 0; u < 8; ++u) {
+                const int k = base + u * 32 + lane;
+                c[u] = k < k1 ? HPR_BATCH_LD(M.ci + k) : 0;
+                v[u] = k < k1 ? HPR_BATCH_LD(M.v + k) : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < kBU; ++u) {
-                const int i = u * 32 + lane;
-                sv[bwin_slot(i)] = p[u];
-                sh[i] = 0;
-            }
+            for (int u = 0; u < 8; ++u) sc[u * 32 + lane] = v[u] * x[c[u]];
             __syncwarp();
-            if (a < e && a >= base && a < nb) sh[a - base] = 1;
-            __syncwarp();
-            double run = lane == 0 ? carry : 0.0;
-            bool seg = false;
-#pragma unroll
-            for (int j = 0; j < kBU; ++j) {
-                const int i = lane * kBU + j;
-                const double q = sv[bwin_slot(i)];
-                if (sh[i]) {
-                    run = q;
-                    seg = true;
-                } else {
-                    run += q;
-                }
-                p[j] = run;
+            const int lo = max(a, base), hi = min(e, base + kWin);
+            double s0 = 0.0, s1 = 0.0;
+            int j = lo;
+            for (; j + 1 < hi; j += 2) {
+                s0 += sc[j - base];
+                s1 += sc[j + 1 - base];
             }
-            double tail = run;
-            bool tseg = seg;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const double tl = __shfl_up_sync(0xffffffffu, tail, off);
-                const bool fl = __shfl_up_sync(0xffffffffu, (int)tseg, off);
-                if (lane >= off && !tseg) {
-                    tail = tl + tail;
-                    tseg = fl;
-                }
-            }
-            double cin = __shfl_up_sync(0xffffffffu, tail, 1);
-            if (lane == 0) cin = 0.0;
-            __syncwarp();
-            bool h = false;
-#pragma unroll
-            for (int j = 0; j < kBU; ++j) {
-                const int i = lane * kBU + j;
-                h = h || sh[i];
-                if (!h) p[j] = cin + p[j];
-                sv[bwin_slot(i)] = p[j];
-            }
-            carry = __shfl_sync(0xffffffffu, p[kBU - 1], 31);
-            __syncwarp();
-            if (a < e && e - 1 >= base && e - 1 < nb) rowsum[lane] = sv[bwin_slot(e - 1 - base)];
+            if (j < hi) s0 += sc[j - base];
+            mine += s0 + s1;
             __syncwarp();
         }
-        if (lane < nr) f(r0 + lane, rowsum[lane]);
+        if (lane < nr) f(r0 + lane, mine);
     }
 }
 
@@ -402,14 +331,14 @@ static __device__ __forceinline__ size_t adaptive_step_d(long long iter)
 __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs B)
 {
     extern __shared__ __align__(16) double dyn_smem[];
-    double *scratch = dyn_smem;  // kScratchDoubles
+    double *scratch = dyn_smem;  // kBW * kWin
     __shared__ CtaState S;
     __shared__ double s_red[kBW][8];
     __shared__ double s_out[8];
     __shared__ int s_inst;
     const int tid = threadIdx.x;
     Vecs V = carve(B.ws + (size_t)blockIdx.x * B.ws_stride, B.nmax, B.mmax,
-                   B.vec_smem ? dyn_smem + kScratchDoubles : nullptr);
+                   B.vec_smem ? dyn_smem + kBW * kWin : nullptr);
 
     for (;;) {
         if (tid == 0) {
@@ -422,9 +351,9 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
         if (k < 0) break;
         const BInst I = B.inst[k];
         const int n = I.n, m = I.m;
-        LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz, B.tiles + I.q_t, I.q_nt};
-        LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz, B.tiles + I.a_t, I.a_nt};
-        LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz, B.tiles + I.at_t, I.at_nt};
+        LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz};
+        LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz};
+        LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz};
         double *qv = B.q_v + I.q_nz, *av = B.a_v + I.a_nz, *atv = B.at_v + I.at_nz;
         const int q_nnz = Q.rp[n], a_nnz = m > 0 ? A.rp[m] : 0;
 
@@ -1083,7 +1012,6 @@ struct AdjArgs {
     const int *order;
     int *counter;
     const int *q_rp, *q_ci, *a_rp, *a_ci, *at_rp, *at_ci;
-    const int2 *tiles;
     const double *q_v, *a_v, *at_v;             // scaled matrices left by the last solve
     const double *col_norm, *row_norm, *z, *y;  // per instance, packed
     const double *gx, *gy;                      // loss gradients (packed; gy may be null)
@@ -1111,7 +1039,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_adjoint(const AdjArgs
     const int tid = threadIdx.x;
     const int na = (B.nmax + 31) & ~31, ma = (B.mmax + 31) & ~31;
     double *g = B.ws + (size_t)blockIdx.x * B.ws_stride;
-    double *lz = B.lanczos_smem ? dyn_smem + kScratchDoubles
+    double *lz = B.lanczos_smem ? dyn_smem + kBW * kWin
                                 : g + kAdjGlobalN * (size_t)na + kAdjGlobalM * (size_t)ma;
     for (;;) {
         if (tid == 0) {
@@ -1124,9 +1052,9 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_adjoint(const AdjArgs
         if (k < 0) break;
         const BInst I = B.inst[k];
         const int n = I.n, m = I.m;
-        const LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz, B.tiles + I.q_t, I.q_nt};
-        const LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz, B.tiles + I.a_t, I.a_nt};
-        const LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz, B.tiles + I.at_t, I.at_nt};
+        const LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz};
+        const LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz};
+        const LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz};
         const double *cn = B.col_norm + I.var, *rn = B.row_norm + I.row;
         const double *zk = B.z + I.var, *yk = B.y + I.row;
         double *sol_n = g, *wo_n = g + na, *w_n = g + 2 * na, *wn_n = g + 3 * na, *tmp = g + 4 * na;
@@ -1448,25 +1376,6 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
     // ---- pack (int32 local indices)
     size_t qnz = 0, anz = 0, qrp = 0, arp = 0, atrp = 0, nv = 0, nr = 0;
     b->inst.resize(K);
-    // SpMV tiles of each matrix: consecutive rows, at most kBTileRows rows and
-    // kBTileCap entries (a longer row is a tile of its own)
-    std::vector<int2> h_tiles;
-    auto plan_tiles = [&](const HPRQPMatrixCSR &Mx, int &first, int &count) {
-        first = (int)h_tiles.size();
-        size_t r = 0;
-        while (r < Mx.nrow) {
-            size_t r1 = r, ent = 0;
-            while (r1 < Mx.nrow && r1 - r < (size_t)kBTileRows) {
-                const size_t l = Mx.row_ptr[r1 + 1] - Mx.row_ptr[r1];
-                if (ent + l > (size_t)kBTileCap && r1 > r) break;
-                ent += l;
-                ++r1;
-            }
-            h_tiles.push_back(make_int2((int)r, (int)r1));
-            r = r1;
-        }
-        count = (int)h_tiles.size() - first;
-    };
     for (size_t k = 0; k < K; ++k) {
         const HPRQPModel &M = b->models[k];
         BInst &I = b->inst[k];
@@ -1481,9 +1390,6 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
         I.n = (int)M.Q.ncol;
         I.m = (int)M.A.nrow;
         I.obj_constant = M.obj_constant;
-        plan_tiles(M.Q, I.q_t, I.q_nt);
-        plan_tiles(M.A, I.a_t, I.a_nt);
-        plan_tiles(M.AT, I.at_t, I.at_nt);
         qnz += M.Q.nnz;
         anz += M.A.nnz;
         qrp += M.Q.nrow + 1;
@@ -1547,8 +1453,7 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
     double *d_qv0, *d_av0, *d_atv0, *d_c, *d_l, *d_u, *d_AL, *d_AU;
     BInst *d_inst;
     int *d_order, *d_counter;
-    int2 *d_tiles;
-    if ((st = balloc(b, &d_tiles, std::max<size_t>(h_tiles.size(), 1))) || (st = balloc(b, &d_qrp, qrp)) || (st = balloc(b, &d_arp, arp)) || (st = balloc(b, &d_atrp, atrp)) ||
+    if ((st = balloc(b, &d_qrp, qrp)) || (st = balloc(b, &d_arp, arp)) || (st = balloc(b, &d_atrp, atrp)) ||
         (st = balloc(b, &d_qci, h_qci.size())) || (st = balloc(b, &d_aci, h_aci.size())) ||
         (st = balloc(b, &d_atci, h_atci.size())) || (st = balloc(b, &d_qv0, h_qv.size())) ||
         (st = balloc(b, &d_av0, h_av.size())) || (st = balloc(b, &d_atv0, h_atv.size())) ||
@@ -1582,15 +1487,12 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
         !up(d_c, h_c.data(), h_c.size() * 8) || !up(d_l, h_l.data(), h_l.size() * 8) ||
         !up(d_u, h_u.data(), h_u.size() * 8) || !up(d_AL, h_AL.data(), h_AL.size() * 8) ||
         !up(d_AU, h_AU.data(), h_AU.size() * 8) || !up(d_inst, b->inst.data(), K * sizeof(BInst)) ||
-        !up(d_order, order.data(), K * sizeof(int)) ||
-        (h_tiles.size() && !up(d_tiles, h_tiles.data(), h_tiles.size() * sizeof(int2))) ||
-        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        !up(d_order, order.data(), K * sizeof(int)) || cudaStreamSynchronize(b->stream) != cudaSuccess)
         return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
     G.inst = d_inst;
     G.order = d_order;
     G.counter = d_counter;
     G.q_rp = d_qrp;
-    G.tiles = d_tiles;
     G.a_rp = d_arp;
     G.at_rp = d_atrp;
     G.q_ci = d_qci;
@@ -1792,7 +1694,6 @@ HPRQPStatus hprqp_batch_backward(HPRQPBatch *b, const double *grad_x, const doub
     A.a_ci = G.a_ci;
     A.at_rp = G.at_rp;
     A.at_ci = G.at_ci;
-    A.tiles = G.tiles;
     A.q_v = G.q_v;
     A.a_v = G.a_v;
     A.at_v = G.at_v;
