@@ -116,6 +116,29 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 # workload
 # --------------------------------------------------------------------------
+def rank_first_instance(rank: int) -> int:
+    """First instance id of a rank's batch: replicas solve disjoint seeded
+    batches (rank r: ids 100000 r ...), so per-GPU work is fixed as N grows."""
+    return 100000 * rank
+
+
+def max_over_ranks(v: float, dist=None, device: str = "cuda") -> float:
+    """Max of a per-rank time over all ranks (every rank calls it in the same
+    order; identity when no process group is initialised)."""
+    if dist is None or not dist.is_initialized():
+        return v
+    import torch
+
+    t = torch.tensor([v], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(per_rank: int, world: int, steps: int, seconds: float) -> float:
+    """Solves/s of the whole job: all ranks' instances over the slowest rank's time."""
+    return per_rank * world * steps / seconds
+
+
 def batch_instances(count: int, start: int = 0):
     from hprqp import instances
 
@@ -393,7 +416,7 @@ def main():
     if args.only == "portfolio":
         print(json.dumps({"portfolio": portfolio_leg()}), flush=True)
         return
-    insts = batch_instances(args.batch, 100000 * rank)
+    insts = batch_instances(args.batch, rank_first_instance(rank))
     packed = hb.pack(insts)
     bytes_algo_per_inst = np.array([bytes_per_iter(i) for i in insts])
     b = hb.Batch(packed, device_number=local_rank)
@@ -402,13 +425,6 @@ def main():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
-
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     for _ in range(args.warmup):
         b.solve(stoptol=STOPTOL)
@@ -423,9 +439,9 @@ def main():
         wall = time.perf_counter() - t0
     launches = hprqp.launch_count() - launches0
     res = b.results(vectors=False)
-    dev_s = max_over_ranks(sum(kernel_ms) / 1e3)
-    wall = max_over_ranks(wall)
-    value = args.batch * world * args.steps / dev_s
+    dev_s = max_over_ranks(sum(kernel_ms) / 1e3, dist)
+    wall = max_over_ranks(wall, dist)
+    value = whole_job_rate(args.batch, world, args.steps, dev_s)
     iters = res.iter.astype(np.float64)
     algo_bytes = float(np.sum(iters * bytes_algo_per_inst))
     achieved = algo_bytes / (statistics.mean(kernel_ms) / 1e3) / 1e9
@@ -444,8 +460,8 @@ def main():
         dt, ok, d2h = e2e_step(packed, local_rank)
         e2e_times.append(dt)
         e2e_ok = ok
-    e2e_s = max_over_ranks(sum(e2e_times))
-    e2e_value = args.batch * world * args.e2e_steps / e2e_s
+    e2e_s = max_over_ranks(sum(e2e_times), dist)
+    e2e_value = whole_job_rate(args.batch, world, args.e2e_steps, e2e_s)
     h2d = int(packed.q_indptr.size * 4 + packed.q_indices.size * 4 + packed.q_data.nbytes +
               2 * (packed.a_indices.size * 4 + packed.a_data.nbytes) + 4 * (packed.a_indptr.size + packed.q_indptr.size)
               + packed.c.nbytes + packed.l.nbytes + packed.u.nbytes + packed.AL.nbytes + packed.AU.nbytes)
