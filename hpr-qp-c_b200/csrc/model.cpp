@@ -323,11 +323,6 @@ HPRQPStatus build_from_QAbc_soc(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A
     return build_from_QAbc(Q, A, c, AL, AU, l, u, obj_constant, model);
 }
 
-HPRQPStatus build_from_mps(const char *mps_path, HPRQPModel *model)
-{
-    (void)mps_path;
-    (void)model;
-    return HPRQP_STATUS_NOT_IMPLEMENTED;
-}
+// build_from_mps lives in mps.cpp
 
 }  // extern "C"

@@ -494,3 +494,83 @@ class RefGpuModel:
             ref_gpu_lib().model_free(ctypes.byref(self.model))
         except Exception:
             pass
+
+
+# --------------------------------------------------------------------------
+# the reference's MPS reader (its CPU library's build_from_mps)
+# --------------------------------------------------------------------------
+
+def _model_arrays(ms) -> dict:
+    def csr(c):
+        nr, nnz = int(c.nrow), int(c.nnz)
+        ip = np.ctypeslib.as_array(c.row_ptr, shape=(nr + 1,)).astype(np.int64).copy()
+        ii = np.ctypeslib.as_array(c.col_ind, shape=(nnz,)).astype(np.int64).copy() if nnz else np.zeros(0, np.int64)
+        dv = np.ctypeslib.as_array(c.values, shape=(nnz,)).copy() if nnz else np.zeros(0)
+        return ip, ii, dv
+
+    n, m = int(ms.Q.ncol), int(ms.A.nrow)
+
+    def vec(ptr, k):
+        return np.ctypeslib.as_array(ptr, shape=(k,)).copy() if (ptr and k) else np.zeros(0)
+
+    q, a = csr(ms.Q), csr(ms.A)
+    return dict(n=n, m=m, q_indptr=q[0], q_indices=q[1], q_data=q[2], a_indptr=a[0], a_indices=a[1], a_data=a[2],
+                c=vec(ms.c, n), l=vec(ms.l, n), u=vec(ms.u, n), AL=vec(ms.AL, m), AU=vec(ms.AU, m),
+                obj_constant=float(ms.obj_constant))
+
+
+_REF_MPS_SCRIPT = r"""
+import ctypes, json, sys
+L = ctypes.CDLL(sys.argv[1])   # loaded before anything else: see ref_build_from_mps
+szp, dp = ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_double)
+class CSR(ctypes.Structure):
+    _fields_ = [("nrow", ctypes.c_size_t), ("ncol", ctypes.c_size_t), ("nnz", ctypes.c_size_t),
+                ("row_ptr", szp), ("col_ind", szp), ("values", dp), ("owns_data", ctypes.c_int)]
+class Model(ctypes.Structure):
+    _fields_ = [("Q", CSR), ("A", CSR), ("AT", CSR), ("c", dp), ("AL", dp), ("AU", dp), ("l", dp), ("u", dp),
+                ("obj_constant", ctypes.c_double), ("owns_data", ctypes.c_int), ("num_var_cones", ctypes.c_size_t),
+                ("var_cone_offsets", szp), ("num_row_cones", ctypes.c_size_t), ("row_cone_offsets", szp),
+                ("soc_rhs", dp)]
+ms = Model()
+L.model_init(ctypes.byref(ms))
+st = L.build_from_mps(sys.argv[2].encode(), ctypes.byref(ms))
+out = {"status": st}
+if st == 0:
+    n, m = ms.Q.ncol, ms.A.nrow
+    h = lambda p, k: [float(p[i]).hex() for i in range(k)]
+    ii = lambda p, k: [int(p[i]) for i in range(k)]
+    out.update(n=n, m=m, q_indptr=ii(ms.Q.row_ptr, n + 1), q_indices=ii(ms.Q.col_ind, ms.Q.nnz),
+               q_data=h(ms.Q.values, ms.Q.nnz), a_indptr=ii(ms.A.row_ptr, m + 1), a_indices=ii(ms.A.col_ind, ms.A.nnz),
+               a_data=h(ms.A.values, ms.A.nnz), c=h(ms.c, n), l=h(ms.l, n), u=h(ms.u, n), AL=h(ms.AL, m),
+               AU=h(ms.AU, m), obj_constant=float(ms.obj_constant).hex())
+    L.model_free(ctypes.byref(ms))
+print("@@" + json.dumps(out))
+"""
+
+
+def ref_build_from_mps(path) -> dict:
+    """Parse an MPS file with the reference's own reader (its CPU library's
+    build_from_mps: src/shared/mps_qp.cpp, mps_reader.cpp) and return its
+    HPRQPModel arrays, or {"status": code}.
+
+    Runs in a fresh interpreter that loads the reference library before any
+    other extension: in a process that has imported numpy first, the
+    reference reader's std::cerr warnings (second objective row, second RHS
+    or BOUNDS set) crashed inside libstdc++ here."""
+    import json as _json
+    import sys as _sys
+
+    r = subprocess.run([_sys.executable, "-c", _REF_MPS_SCRIPT, str(REF_CPU_LIB), str(path)],
+                       capture_output=True, text=True, timeout=120)
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("@@")]
+    if not line:
+        return {"status": -1, "stderr": r.stderr[-2000:]}
+    d = _json.loads(line[0][2:])
+    if d["status"] != 0:
+        return {"status": int(d["status"])}
+    out = {"status": 0, "n": d["n"], "m": d["m"], "obj_constant": float.fromhex(d["obj_constant"])}
+    for k in ("q_indptr", "q_indices", "a_indptr", "a_indices"):
+        out[k] = np.asarray(d[k], np.int64)
+    for k in ("q_data", "a_data", "c", "l", "u", "AL", "AU"):
+        out[k] = np.array([float.fromhex(v) for v in d[k]], np.float64)
+    return out
