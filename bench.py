@@ -169,6 +169,36 @@ def _ref_worker(args):
     return statuses
 
 
+def _ref_single_core(_):
+    """One core, reference CPU library (or the oracle port): the n=1000 QP to
+    1e-6 and 16 members of the differentiation batch (n=500, m=300) to 1e-8."""
+    import pyoracle
+    from hprqp import instances
+
+    def solve(inst, tol):
+        if pyoracle.ref_available():
+            return pyoracle.ref_solve(inst, stoptol=tol)
+        return pyoracle.OracleModel(inst).solve(stoptol=tol, mode=pyoracle.MODE_CPU_REF)
+
+    inst = instances.config0()
+    t0 = time.perf_counter()
+    r = solve(inst, 1e-6)
+    c0 = time.perf_counter() - t0
+    sample = [instances.config4_instance(i) for i in range(16)]
+    t0 = time.perf_counter()
+    st4 = [int(solve(i, 1e-8)["status"]) for i in sample]
+    c4 = (time.perf_counter() - t0) / len(sample)
+    return {"plain_qp_n1000_s": round(c0, 4), "plain_qp_status": int(r["status"]),
+            "diff_batch_member_s": round(c4, 4), "diff_batch_sample": len(sample),
+            "diff_batch_optimal": int(sum(s == 6 for s in st4)), "cores": 1}
+
+
+def cpu_single_core_timings():
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        return pool.map(_ref_single_core, [0])[0]
+
+
 def cpu_reference_rate(ids, cores: int):
     """Reference CPU solves/s over the given batch instances on `cores`
     spawned processes."""
@@ -502,7 +532,8 @@ def main():
         ids = list(range(min(args.cpu_sample, args.batch)))
         rate, kind, cdt, _ = cpu_reference_rate(ids, cores)
         line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind,
-                                "sample": f"{len(ids)} batch instances, one process per core"}
+                                "sample": f"{len(ids)} batch instances, one process per core",
+                                "single_core": cpu_single_core_timings()}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
