@@ -42,10 +42,10 @@ sys.path.insert(0, str(ROOT / "hpr-qp-c_b200" / "python"))
 sys.path.insert(0, str(ROOT / "oracle"))
 
 # DRAM bytes moved per algorithmic byte by k_batch_solve: ncu on a 148-QP
-# launch of this workload read+wrote 43.161 GB (dram__bytes_read.sum +
+# launch of this workload read+wrote 41.152 GB (dram__bytes_read.sum +
 # dram__bytes_write.sum) for 231.757 GB of algorithmic bytes; each
 # instance's matrices stay in L2 across its iterations.
-BATCH_DRAM_PER_ALGO_BYTE = 43.161e9 / 231.757e9
+BATCH_DRAM_PER_ALGO_BYTE = 41.152e9 / 231.757e9
 METRIC = "solves/s to 1e-6 rel-KKT, batched vs plain on 1 B200; SpMV GB/s vs HBM peak"
 STOPTOL = 1e-6
 BATCH = 4096

@@ -582,9 +582,10 @@ def model_arrays(model: Model):
 
 
 def __getattr__(name):
-    """``hprqp.QPFunction`` / ``hprqp.QPLayer``: the differentiable batched
-    layer (imported on first use so that torch stays optional)."""
-    if name in ("QPFunction", "QPLayer"):
+    """``hprqp.QPFunction`` / ``hprqp.QPLayer`` (batched) and
+    ``hprqp.SingleQPFunction`` (one large QP): the differentiable layers,
+    imported on first use so that torch stays optional."""
+    if name in ("QPFunction", "QPLayer", "SingleQPFunction"):
         from . import torch_layer
 
         return getattr(torch_layer, name)
@@ -592,7 +593,7 @@ def __getattr__(name):
 
 
 __all__ = [
-    "QPFunction", "QPLayer", "SolveState", "solve_for_backward", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
+    "QPFunction", "QPLayer", "SingleQPFunction", "SolveState", "solve_for_backward", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
     "STATUS_ALLOCATION_FAILED", "STATUS_CONTINUE", "STATUS_INVALID_ARGUMENT", "STATUS_MAX_ITER",
     "STATUS_NOT_IMPLEMENTED", "STATUS_OK", "STATUS_OPTIMAL", "STATUS_TIME_LIMIT", "build_from_mps",
     "build_from_QAbc", "build_from_qabc", "build_from_instance", "gpu_backend_available", "optimize",

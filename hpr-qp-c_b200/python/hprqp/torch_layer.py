@@ -77,6 +77,72 @@ class QPFunction(torch.autograd.Function):
         return (None, None, None, t(g.dQ), t(g.dA), t(g.dc), t(g.dAL), t(g.dAU), t(g.dl), t(g.du))
 
 
+class SingleQPFunction(torch.autograd.Function):
+    """One (large) QP through solve_gpu + the device-wide adjoint
+    (hprqp_diff.h).  ``SingleQPFunction.apply(structure, solve_kw,
+    backward_tol, q_data, a_data, c, AL, AU, l, u) -> (x, y)`` with
+    ``structure = (n, m, q_indptr, q_indices, a_indptr, a_indices)`` (CSR
+    index arrays of the caller's Q and A); y has one entry per caller row
+    (rows removed by preprocessing -- empty, or free on both sides -- get 0)."""
+
+    @staticmethod
+    def forward(ctx, structure, solve_kw: dict, backward_tol: float, q_data, a_data, c, AL, AU, l, u):
+        from . import Parameters, build_from_qabc, solve_for_backward
+        import scipy.sparse as sp
+
+        n, m, qi, qj, ai, aj = structure
+        qv, av = _np(q_data), _np(a_data)
+        Q = sp.csr_matrix((qv, qj, qi), shape=(n, n))
+        A = sp.csr_matrix((av, aj, ai), shape=(m, n))
+        ALn, AUn = _np(AL), _np(AU)
+        model = build_from_qabc(Q, _np(c), A, ALn, AUn, _np(l), _np(u))
+        kw = dict(solve_kw)
+        r, state = solve_for_backward(model, Parameters(verbose=False, **kw))
+        if state is None:
+            raise RuntimeError(f"hprqp SingleQPFunction: solve ended with status {r.status}")
+        lens = np.diff(np.asarray(ai))
+        kept = np.nonzero((lens > 0) & ~(np.isneginf(ALn) & np.isposinf(AUn)))[0]
+        if len(kept) != len(r.y):
+            state.close()
+            raise RuntimeError("hprqp SingleQPFunction: unexpected row preprocessing")
+        y = np.zeros(m)
+        y[kept] = r.y
+        ctx.state, ctx.model, ctx.kept, ctx.tol = state, model, kept, backward_tol
+        ctx.x, ctx.y, ctx.structure, ctx.device = r.x, y, structure, c.device
+        return torch.from_numpy(r.x.copy()).to(c.device), torch.from_numpy(y).to(c.device)
+
+    @staticmethod
+    def backward(ctx, gx, gy):
+        state = getattr(ctx, "state", None)
+        if state is None:
+            raise RuntimeError("hprqp SingleQPFunction: backward called twice (retain_graph is not supported)")
+        n, m, qi, qj, ai, aj = ctx.structure
+        gxn = _np(gx) if gx is not None else np.zeros(n)
+        gyk = _np(gy)[ctx.kept] if gy is not None else None
+        try:
+            g = state.backward(gxn, gyk, tol=ctx.tol)
+        finally:
+            state.close()
+            ctx.state = None
+        lam = g["lam"]
+        mu = np.zeros(m)
+        mu[ctx.kept] = g["mu"]
+        x, y = ctx.x, ctx.y
+        qrow = np.repeat(np.arange(n), np.diff(np.asarray(qi)))
+        qcol = np.asarray(qj)
+        arow = np.repeat(np.arange(m), np.diff(np.asarray(ai)))
+        acol = np.asarray(aj)
+        dQ = -0.5 * (lam[qrow] * x[qcol] + lam[qcol] * x[qrow])
+        dA = -mu[arow] * x[acol] + lam[acol] * y[arow]
+        dAL = np.zeros(m)
+        dAU = np.zeros(m)
+        dAL[ctx.kept] = g["dAL"]
+        dAU[ctx.kept] = g["dAU"]
+        dev = ctx.device
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        return (None, None, None, t(dQ), t(dA), t(g["dc"]), t(dAL), t(dAU), t(g["dl"]), t(g["du"]))
+
+
 class QPLayer(torch.nn.Module):
     """Batched QP layer.  ``structure`` fixes the offsets and the CSR index
     arrays of Q and A (its numeric arrays are ignored); ``forward`` takes the

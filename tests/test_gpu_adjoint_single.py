@@ -128,3 +128,40 @@ def test_single_adjoint_large_kkt_residual(engine_lib):
     sol = np.concatenate([g["lam"][F], g["mu"][R]])
     assert np.linalg.norm(K @ sol - rhs) <= 1e-8 * np.linalg.norm(rhs)
     assert np.all(g["lam"][r.z != 0.0] == 0.0) and np.all(g["mu"][r.y == 0.0] == 0.0)
+
+
+def test_torch_single_qp_function_matches_batched_layer(engine_lib):
+    """hprqp.SingleQPFunction (solve_gpu + device-wide adjoint) and the
+    batched QPFunction give the same gradients for the same QP, on CUDA
+    tensors; a row removed by preprocessing gets zero gradients."""
+    import torch
+
+    import hprqp
+    from hprqp import batch
+
+    inst = instances.adjoint_case(2)
+    # add an empty row (removed by preprocessing) at the end
+    A = inst.A
+    inst.A = instances.CSR(A.nrow + 1, A.ncol, np.append(A.indptr, A.indptr[-1]), A.indices, A.data)
+    inst.AL = np.append(inst.AL, -1.0)
+    inst.AU = np.append(inst.AU, 1.0)
+    dev = "cuda"
+    t = lambda a: torch.tensor(np.asarray(a, float), dtype=torch.float64, device=dev, requires_grad=True)  # noqa
+    rng = np.random.default_rng(21)
+    wx = torch.tensor(rng.standard_normal(inst.n), device=dev)
+    wy = torch.tensor(rng.standard_normal(inst.m), device=dev)
+    grads = []
+    for which in ("single", "batched"):
+        tensors = [t(v) for v in (inst.Q.data, inst.A.data, inst.c, inst.AL, inst.AU, inst.l, inst.u)]
+        if which == "single":
+            structure = (inst.n, inst.m, inst.Q.indptr, inst.Q.indices, inst.A.indptr, inst.A.indices)
+            x, y = hprqp.SingleQPFunction.apply(structure, {"stoptol": 1e-11}, 1e-13, *tensors)
+        else:
+            layer = hprqp.QPLayer(batch.pack([inst]), backward_tol=1e-13, stoptol=1e-11)
+            x, y = layer(*tensors)
+        ((wx * x).sum() + (wy * y).sum()).backward()
+        grads.append([tt.grad.cpu().numpy() for tt in tensors])
+        assert float(y[-1]) == 0.0
+    for gs, gb in zip(*grads):
+        assert _close(gs, gb, 1e-6)
+    assert grads[0][3][-1] == 0.0 and grads[0][4][-1] == 0.0  # dAL, dAU of the removed row

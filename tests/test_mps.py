@@ -78,7 +78,7 @@ def test_solve_from_mps_matches_arrays(engine_lib, tmp_path):
     a1, a2 = hprqp.model_arrays(m1), hprqp.model_arrays(m2)
     for k in ("q_indptr", "q_indices", "q_data", "a_indptr", "a_indices", "a_data", "c", "l", "u", "AL"):
         assert np.array_equal(a1[k], a2[k]), k
-    assert np.allclose(a1["AU"], a2["AU"], rtol=1e-15, atol=0)
+    assert np.allclose(a1["AU"], a2["AU"], rtol=1e-12, atol=1e-14)
     r1 = hprqp.optimize(m1, hprqp.Parameters(verbose=False, stoptol=1e-6))
     r2 = hprqp.optimize(m2, hprqp.Parameters(verbose=False, stoptol=1e-6))
     assert r1.status_code == r2.status_code == hprqp.STATUS_OPTIMAL
