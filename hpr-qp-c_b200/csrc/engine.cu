@@ -1831,6 +1831,47 @@ HPRQPStatus engine_adjoint(Engine *e, const double *gx, const double *gy, double
     return HPRQP_STATUS_OK;
 }
 
+// ---- caller-given iterate (diagnostics) ---------------------------------------
+struct EpiSetBars : EpiBase<0> {  // scaled space: x_bar = x cn, z_bar = z / cn, y_bar = y rn
+    int n, m;
+    const double *x, *y, *z, *cn, *rn;
+    double *xb, *yb, *zb;
+    __device__ void row(int i, double, Acc<0> &) const
+    {
+        if (i < n) {
+            xb[i] = x[i] * cn[i];
+            zb[i] = z[i] / cn[i];
+        }
+        if (i < m) yb[i] = y[i] * rn[i];
+    }
+};
+
+HPRQPStatus engine_set_bars(Engine *e, const double *x, const double *y, const double *z)
+{
+    DState &S = e->S;
+    const int n = S.n, m = S.m;
+    double *buf = nullptr;
+    HPRQPStatus st = dalloc(e, &buf, (size_t)2 * std::max(n, 1) + std::max(m, 1));
+    if (st) return st;
+    if (n) HPR_CK(cudaMemcpyAsync(buf, x, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    if (n) HPR_CK(cudaMemcpyAsync(buf + n, z, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    if (m) HPR_CK(cudaMemcpyAsync(buf + 2 * (size_t)n, y, m * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    EpiSetBars sb;
+    sb.n = n;
+    sb.m = m;
+    sb.x = buf;
+    sb.z = buf + n;
+    sb.y = buf + 2 * (size_t)n;
+    sb.cn = S.col_norm;
+    sb.rn = S.row_norm;
+    sb.xb = S.x_bar;
+    sb.yb = S.y_bar;
+    sb.zb = S.z_bar;
+    launch_ew(e, std::max(n, m), sb);
+    HPR_CK(cudaStreamSynchronize(e->stream));
+    return HPRQP_STATUS_OK;
+}
+
 HPRQPStatus engine_dump_scaling(Engine *e, ScaleDump *d)
 {
     DState &S = e->S;
@@ -1963,6 +2004,21 @@ HPRQPStatus hprqp_b200_setup(const HPRQPModel *model, const HPRQPParams *params,
     out9[8] = info.scaling_scalars.norm_c;
     hpr::ScaleDump d{row_norm, col_norm, q_val, a_val, at_val, c, l, u, AL, AU, 0, 0, 0, 0};
     st = hpr::engine_dump_scaling(e, &d);
+    hpr::engine_destroy(e);
+    return st;
+}
+
+HPRQPStatus hprqp_b200_residuals(const HPRQPModel *model, const HPRQPParams *params, const double *x,
+                                 const double *y, const double *z, size_t iter, HPRQPResiduals *out)
+{
+    if (!model || !params || !x || !z || !out || (model->A.nrow > 0 && !y)) return HPRQP_STATUS_INVALID_ARGUMENT;
+    hpr::Engine *e = nullptr;
+    hpr::SetupInfo info;
+    memset(&info, 0, sizeof(info));
+    HPRQPStatus st = hpr::engine_create(model, params, &e, &info);
+    if (st != HPRQP_STATUS_OK) return st;
+    st = hpr::engine_set_bars(e, x, y, z);
+    if (st == HPRQP_STATUS_OK) st = hpr::engine_residuals(e, out, iter);
     hpr::engine_destroy(e);
     return st;
 }

@@ -45,6 +45,10 @@ struct ScaleDump {
 };
 HPRQPStatus engine_dump_scaling(Engine *e, ScaleDump *d);
 
+// Replace the engine's (x_bar, y_bar, z_bar) by a caller-given iterate in
+// original space (host arrays; scaled on the device).
+HPRQPStatus engine_set_bars(Engine *e, const double *x, const double *y, const double *z);
+
 // Implicit-differentiation adjoint of the finished solve held by e: MINRES
 // on the scaled active-set KKT operator (variables with z_bar == 0, rows with
 // y_bar != 0).  gx (n) and gy (m, may be NULL) are host arrays in the model's

@@ -427,6 +427,34 @@ def optimize(model: Model, params: Optional[Parameters] = None, as_numpy: bool =
         lib.hprqp_results_destroy(results_handle)
 
 
+class _ResidualsStruct(ctypes.Structure):
+    _fields_ = [("is_updated", ctypes.c_int), ("err_Rp_org_bar", ctypes.c_double),
+                ("err_Rd_org_bar", ctypes.c_double), ("KKTx_and_gap_org_bar", ctypes.c_double),
+                ("primal_obj_bar", ctypes.c_double), ("rel_gap_bar", ctypes.c_double),
+                ("dual_obj_bar", ctypes.c_double)]
+
+
+def residuals(model: Model, x, y, z, iter: int = 1, params: Optional[Parameters] = None) -> dict:
+    """The solver's residual kernels at a given point of the preprocessed
+    model (hprqp_b200_residuals): errRp, errRd, gap, objectives, KKT."""
+    if params is None:
+        params = Parameters(verbose=False)
+    n, m = model.num_variables, model.num_constraints
+    xa = np.ascontiguousarray(np.broadcast_to(np.asarray(x, np.float64), (n,)))
+    za = np.ascontiguousarray(np.broadcast_to(np.asarray(z, np.float64), (n,)))
+    ya = np.ascontiguousarray(np.broadcast_to(np.asarray(y, np.float64), (m,))) if m else np.zeros(1)
+    out = _ResidualsStruct()
+    lib = _lib()
+    lib.hprqp_b200_residuals.argtypes = [ctypes.c_void_p, ctypes.c_void_p, c_double_p, c_double_p, c_double_p,
+                                         ctypes.c_size_t, ctypes.POINTER(_ResidualsStruct)]
+    lib.hprqp_b200_residuals.restype = ctypes.c_int
+    _raise_for_status(lib.hprqp_b200_residuals(model._handle, params._handle, xa.ctypes.data_as(c_double_p),
+                                               ya.ctypes.data_as(c_double_p), za.ctypes.data_as(c_double_p),
+                                               int(iter), ctypes.byref(out)), "hprqp_b200_residuals")
+    return {"err_rp": out.err_Rp_org_bar, "err_rd": out.err_Rd_org_bar, "gap": out.rel_gap_bar,
+            "primal_obj": out.primal_obj_bar, "dual_obj": out.dual_obj_bar, "kkt": out.KKTx_and_gap_org_bar}
+
+
 class _ResultsStruct(ctypes.Structure):
     _fields_ = [("iter", ctypes.c_size_t), ("iter_4", ctypes.c_size_t), ("iter_6", ctypes.c_size_t),
                 ("time", ctypes.c_double), ("time_4", ctypes.c_double), ("time_6", ctypes.c_double),
@@ -593,7 +621,7 @@ def __getattr__(name):
 
 
 __all__ = [
-    "QPFunction", "QPLayer", "SingleQPFunction", "SolveState", "solve_for_backward", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
+    "QPFunction", "QPLayer", "SingleQPFunction", "SolveState", "residuals", "solve_for_backward", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
     "STATUS_ALLOCATION_FAILED", "STATUS_CONTINUE", "STATUS_INVALID_ARGUMENT", "STATUS_MAX_ITER",
     "STATUS_NOT_IMPLEMENTED", "STATUS_OK", "STATUS_OPTIMAL", "STATUS_TIME_LIMIT", "build_from_mps",
     "build_from_QAbc", "build_from_qabc", "build_from_instance", "gpu_backend_available", "optimize",

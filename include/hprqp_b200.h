@@ -29,6 +29,14 @@ HPRQPStatus hprqp_b200_spmv(size_t nrow, size_t ncol, size_t nnz, const size_t *
                             const size_t *col_ind, const double *values, const double *x, double *y,
                             int reps, double *ms_per_spmv);
 
+/* The solver's residual kernels at a caller-given point (x, y, z) in the
+ * original space of the preprocessed model (x, z: n entries, y: m): setup as
+ * solve_gpu performs it, then the fused residual SpMVs and reductions
+ * (reference gpu_compute_residuals_value, src/gpu/residuals.cu:81-183);
+ * iter == 0 adds the bound-violation term to errRp as at the first check. */
+HPRQPStatus hprqp_b200_residuals(const HPRQPModel *model, const HPRQPParams *params, const double *x,
+                                 const double *y, const double *z, size_t iter, HPRQPResiduals *out);
+
 /* Setup of a model exactly as solve_gpu performs it (upload, Ruiz x10 +
  * Pock-Chambolle scaling, Q-diagonal test, power iterations, sigma0).
  * out[0..4] = sigma0, lambda_max_A, lambda_max_Q, Q_is_diag, noC;

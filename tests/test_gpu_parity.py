@@ -162,3 +162,37 @@ def test_max_iter_zero_and_invalid_device(engine_lib):
     assert r.status_code == hprqp.STATUS_MAX_ITER and len(r.x) == 2
     r = hprqp.optimize(model, hprqp.Parameters(verbose=False, device_number=999))
     assert r.status_code == hprqp.STATUS_INVALID_ARGUMENT
+
+
+def test_residual_kernels_known_answers(engine_lib):
+    """The residual kernels at seeded points of the reference's residual
+    fixture (tests/gpu/test_gpu_residuals.c:72-89 of the reference): pobj 3,
+    dobj -1, errRd 0.46, errRp 0, gap 1, KKT 1; at iteration 0 the bound
+    violation of x = (11, 1) gives errRp 1."""
+    hprqp = engine_lib
+    inst = {i.name: i for i in instances.tiny_cases()}["residuals"]
+    model = hprqp.build_from_instance(inst)
+    params = hprqp.Parameters(verbose=False, use_scaling=False)
+    r = hprqp.residuals(model, [1.0, 1.0], [0.5], [0.2, 0.3], iter=1, params=params)
+    for key, want in (("primal_obj", 3.0), ("dual_obj", -1.0), ("err_rd", 0.46), ("err_rp", 0.0), ("gap", 1.0),
+                      ("kkt", 1.0)):
+        assert abs(r[key] - want) <= 1e-8, (key, r[key])
+    r0 = hprqp.residuals(model, [11.0, 1.0], [0.0], [0.0, 0.0], iter=0, params=params)
+    assert abs(r0["err_rp"] - 1.0) <= 1e-8
+
+
+@pytest.mark.parametrize("scaling", [True, False])
+def test_residual_kernels_match_oracle(engine_lib, scaling):
+    """At a random point of the n=1000 QP, with and without scaling, the
+    device residuals agree with the oracle's FP64 host recomputation."""
+    hprqp = engine_lib
+    inst = instances.config0()
+    model = hprqp.build_from_instance(inst)
+    rng = np.random.default_rng(8)
+    x = rng.uniform(-2, 2, inst.n)
+    y = rng.standard_normal(inst.m)
+    z = rng.standard_normal(inst.n)
+    r = hprqp.residuals(model, x, y, z, iter=5, params=hprqp.Parameters(verbose=False, use_scaling=scaling))
+    k = pyoracle.OracleModel(inst).kkt(x, y, z)
+    for key in ("err_rp", "err_rd", "gap", "primal_obj", "dual_obj"):
+        assert abs(r[key] - k[key]) <= 1e-10 * max(1.0, abs(k[key])), (key, r[key], k[key])
