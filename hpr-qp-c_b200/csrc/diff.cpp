@@ -5,6 +5,7 @@
 #include "hprqp_diff.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <cstring>
 #include <thread>
@@ -73,6 +74,10 @@ HPRQPStatus hprqp_backward(HPRQPSolveState *s, const double *grad_x, const doubl
     if (!s || !s->eng || !grad_x || !g) return HPRQP_STATUS_INVALID_ARGUMENT;
     const auto t0 = std::chrono::steady_clock::now();
     const HPRQPModel &M = *s->model;
+    if (M.num_var_cones || M.num_row_cones) {
+        fprintf(stderr, "hprqp-b200: hprqp_backward does not differentiate through second-order cones\n");
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
+    }
     const size_t n = M.Q.ncol, m = M.A.nrow;
     if (!(tol > 0.0)) tol = 1e-12;
     if (max_iter <= 0) max_iter = 4 * (long long)(n + m) + 100;

@@ -81,6 +81,10 @@ struct DState {
         *last_x, *last_y, *last_Qw, *last_w, *last_ATy;
     double *pz, *pq, *ptmp, *fac_r, *fac_c;  // setup scratch
     Ctl *ctl;
+    // second-order cones (0 when none): cone offsets, linear lengths, scaled rhs
+    int nvc = 0, nrc = 0, lin_n = 0, lin_m = 0;
+    int *vco = nullptr, *rco = nullptr;
+    double *rhs = nullptr;
 };
 
 struct Scal {
@@ -291,6 +295,151 @@ struct EpiQwNoC : EpiBase<0> {
 struct EpiStore : EpiBase<0> {
     double *out;
     __device__ void row(int i, double v, Acc<0> &) const { out[i] = v; }
+};
+
+// ---- second-order cones (reference src/gpu/soc_common.cuh,
+// soc_iteration.cuh, soc_residuals.cuh) ------------------------------------
+// Cones are contiguous suffix blocks: variables [vco[0], n), rows [rco[0], m).
+
+// out = projection of in onto [lo, up] on [0, lin) and onto the Lorentz
+// cones {(t, v) : |v| <= t} of the blocks; one warp per cone, the norm of v
+// taken as max|v| * sqrt(sum (v_j / max|v|)^2) so squares cannot overflow.
+__global__ void k_soc_project(const double *in, double *out, const double *lo, const double *up, int lin,
+                              const int *off, int ncones)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    for (int i = tid; i < lin; i += nth) out[i] = clampd(in[i], lo[i], up[i]);
+    const int lane = threadIdx.x & 31, wid = tid >> 5, nw = nth >> 5;
+    for (int k = wid; k < ncones; k += nw) {
+        const int b = off[k], e = off[k + 1];
+        const double t = in[b];
+        double mx = 0.0;
+        for (int j = b + 1 + lane; j < e; j += 32) mx = fmax(mx, fabs(in[j]));
+        mx = warp_max(mx);
+        double sum = 0.0;
+        if (mx > 0.0)
+            for (int j = b + 1 + lane; j < e; j += 32) {
+                const double q = in[j] / mx;
+                sum += q * q;
+            }
+        sum = warp_sum(sum);
+        const double nrm = mx * sqrt(sum);
+        if (nrm <= t) {
+            for (int j = b + lane; j < e; j += 32) out[j] = in[j];
+        } else if (nrm <= -t) {
+            for (int j = b + lane; j < e; j += 32) out[j] = 0.0;
+        } else {
+            const double alpha = 0.5 + 0.5 * (t / nrm);
+            if (lane == 0) out[b] = 0.5 * nrm + 0.5 * t;
+            for (int j = b + 1 + lane; j < e; j += 32) out[j] = alpha * in[j];
+        }
+    }
+}
+
+// scaling factors: the block maximum on every cone, so that a positive scalar
+// scales each cone (which leaves the cone invariant)
+__global__ void k_cone_block_max(double *f, const int *off, int ncones)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31, wid = tid >> 5, nw = nth >> 5;
+    for (int k = wid; k < ncones; k += nw) {
+        double mx = 0.0;
+        for (int j = off[k] + lane; j < off[k + 1]; j += 32) mx = fmax(mx, f[j]);
+        mx = warp_max(mx);
+        for (int j = off[k] + lane; j < off[k + 1]; j += 32) f[j] = mx;
+    }
+}
+
+// S1: Qw = Q w; tempv = x + sigma (-Qw + A'y - c) (the point to project)
+struct EpiSocX1 : EpiBase<0> {
+    DState S;
+    __device__ void row(int i, double qw, Acc<0> &) const
+    {
+        const double sigma = S.ctl->sigma;
+        S.Qw[i] = qw;
+        S.tempv[i] = S.x[i] + sigma * (-qw + S.ATy[i] - S.c[i]);
+    }
+    __device__ void extra(Acc<0> &) const { latch_inner(S.ctl); }
+};
+
+// S3 (over n): x_bar = proj(tempv) is in place; z_bar, x_hat, Halpern x, w_bar
+struct EpiSocXFinish : EpiBase<0> {
+    DState S;
+    __device__ void row(int i, double, Acc<0> &) const
+    {
+        const Scal k = load_scal(S.ctl, false);
+        const double x = S.x[i], xb = S.x_bar[i], xh = 2.0 * xb - x;
+        const double f2 = S.q_is_diag ? S.fact2[i] : 1.0 / (1.0 + k.sigma * k.lQ);
+        const double f1 = S.q_is_diag ? S.fact1[i] : 1.0 - f2;
+        S.dx[i] = xb - x;
+        S.z_bar[i] = (xb - S.tempv[i]) / k.sigma;
+        S.x_hat[i] = xh;
+        S.x[i] = k.h1 * S.last_x[i] + k.h2 * xh;
+        S.w_bar[i] = f1 * S.w[i] + f2 * xh;
+    }
+};
+
+// S5: Ax = A tempv; Rp = Ax - rhs - tau y (the point to project), in pz
+struct EpiSocY1 : EpiBase<0> {
+    DState S;
+    __device__ void row(int i, double ax, Acc<0> &) const
+    {
+        const double tau = S.ctl->sigma * S.ctl->lambda_A;
+        S.Ax[i] = ax;
+        S.pz[i] = ax - (S.rhs ? S.rhs[i] : 0.0) - tau * S.y[i];
+    }
+};
+
+// S7 (over m): s = proj(Rp) is in place; y_bar, dy, Halpern y
+struct EpiSocYFinish : EpiBase<0> {
+    DState S;
+    __device__ void row(int i, double, Acc<0> &) const
+    {
+        const Scal k = load_scal(S.ctl, false);
+        const double tau = k.sigma * k.lA;
+        const double y = S.y[i], yb = (S.s[i] - S.pz[i]) / tau;
+        S.dy[i] = yb - y;
+        S.y_bar[i] = yb;
+        S.y[i] = k.h1 * S.last_y[i] + k.h2 * (2.0 * yb - y);
+    }
+};
+
+// residuals: A x_bar - rhs into pq; slot: max|Ax rs|
+struct EpiSocResA : EpiBase<1> {
+    DState S;
+    __host__ __device__ void ops(int *o) const { o[0] = kMax; }
+    __device__ void row(int i, double ax, Acc<1> &a) const
+    {
+        S.pq[i] = ax - (S.rhs ? S.rhs[i] : 0.0);
+        a.v[0] = fmax(a.v[0], fabs(ax * S.row_norm[i]));
+    }
+};
+
+// residuals (over m): proj(Ax - rhs) is in pz; slots: max|Rp|, y_bar.s, y_bar.rhs
+struct EpiSocRp : EpiBase<3> {
+    DState S;
+    __host__ __device__ void ops(int *o) const
+    {
+        o[0] = kMax;
+        o[1] = kSum;
+        o[2] = kSum;
+    }
+    __device__ void row(int i, double, Acc<3> &a) const
+    {
+        a.v[0] = fmax(a.v[0], fabs((S.pz[i] - S.pq[i]) * S.row_norm[i]));
+        a.v[1] += S.y_bar[i] * S.s[i];
+        if (S.rhs) a.v[2] += S.y_bar[i] * S.rhs[i];
+    }
+};
+
+// residuals (over n): proj(x_bar) is in ptmp; slot: max|proj - x_bar| / cs
+struct EpiSocViol : EpiBase<1> {
+    DState S;
+    __host__ __device__ void ops(int *o) const { o[0] = kMax; }
+    __device__ void row(int i, double, Acc<1> &a) const
+    {
+        a.v[0] = fmax(a.v[0], fabs((S.ptmp[i] - S.x_bar[i]) / S.col_norm[i]));
+    }
 };
 
 // ---- residuals (reference src/gpu/residuals.cu:81-183) ---------------------
@@ -704,6 +853,7 @@ __global__ void k_apply_m(const DState S, const double *cf, const double *rf)
             S.row_norm[r] *= rf[r];
             S.AL[r] /= rf[r];
             S.AU[r] /= rf[r];
+            if (S.rhs) S.rhs[r] /= rf[r];
         }
     }
 }
@@ -1149,6 +1299,31 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
         E_CK(cudaMemcpyAsync(S.AL, model->AL, m * sizeof(double), cudaMemcpyHostToDevice, e->stream));
         E_CK(cudaMemcpyAsync(S.AU, model->AU, m * sizeof(double), cudaMemcpyHostToDevice, e->stream));
     }
+    // second-order cones: offsets (int), linear lengths, rhs
+    S.lin_n = n;
+    S.lin_m = m;
+    if (model->num_var_cones || model->num_row_cones) {
+        auto up_off = [&](const size_t *off, size_t count, int **dst) -> HPRQPStatus {
+            std::vector<int> h(count + 1);
+            for (size_t k = 0; k <= count; ++k) h[k] = (int)off[k];
+            HPRQPStatus st2 = dalloc(e, dst, count + 1);
+            if (st2) return st2;
+            HPR_CK(cudaMemcpy(*dst, h.data(), (count + 1) * sizeof(int), cudaMemcpyHostToDevice));
+            return HPRQP_STATUS_OK;
+        };
+        if (model->num_var_cones) {
+            E_ST(up_off(model->var_cone_offsets, model->num_var_cones, &S.vco));
+            S.nvc = (int)model->num_var_cones;
+            S.lin_n = (int)model->var_cone_offsets[0];
+        }
+        if (model->num_row_cones) {
+            E_ST(up_off(model->row_cone_offsets, model->num_row_cones, &S.rco));
+            S.nrc = (int)model->num_row_cones;
+            S.lin_m = (int)model->row_cone_offsets[0];
+            E_ST(dalloc(e, &S.rhs, (size_t)m));
+            E_CK(cudaMemcpy(S.rhs, model->soc_rhs, m * sizeof(double), cudaMemcpyHostToDevice));
+        }
+    }
     {
         std::vector<double> ones(nmax, 1.0);
         E_CK(cudaMemcpyAsync(S.col_norm, ones.data(), n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
@@ -1167,6 +1342,8 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
         E_ST(finalize(e, &f, 1, true));
     }
     e->norm_b_org = m > 0 ? e->hout->v[0] : 0.0;
+    if (S.rhs)
+        for (int r = 0; r < m; ++r) e->norm_b_org = std::max(e->norm_b_org, std::fabs(model->soc_rhs[r]));
     e->norm_c_org = e->hout->v[2];
     e->obj_constant = model->obj_constant;
     info->scaling_scalars.norm_b_org = e->norm_b_org;
@@ -1179,6 +1356,14 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
             count_launch();
             if (m > 0) {
                 k_row_factors<<<wgrid, kThreads, 0, e->stream>>>(S, use_sum, S.fac_r);
+                count_launch();
+            }
+            if (S.nvc) {
+                k_cone_block_max<<<wgrid, kThreads, 0, e->stream>>>(S.fac_c, S.vco, S.nvc);
+                count_launch();
+            }
+            if (S.nrc) {
+                k_cone_block_max<<<wgrid, kThreads, 0, e->stream>>>(S.fac_r, S.rco, S.nrc);
                 count_launch();
             }
             k_apply_n<<<wgrid, kThreads, 0, e->stream>>>(S, S.fac_c, S.fac_r);
@@ -1196,8 +1381,15 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
         E_ST(finalize(e, &f, 1, true));
     }
     HPR_TRACE("create: scaled");
-    const double norm_b = m > 0 ? sqrt(e->hout->v[1]) : 0.0;
+    double norm_b = m > 0 ? sqrt(e->hout->v[1]) : 0.0;
     const double norm_c = sqrt(e->hout->v[3]);
+    if (S.rhs) {
+        std::vector<double> rs(m), rn(m);
+        E_CK(cudaMemcpy(rs.data(), S.rhs, m * sizeof(double), cudaMemcpyDeviceToHost));
+        double ss = 0.0;
+        for (int r = 0; r < m; ++r) ss += rs[r] * rs[r];
+        norm_b = std::max(norm_b, sqrt(ss));
+    }
     info->scaling_scalars.norm_b = norm_b;
     info->scaling_scalars.norm_c = norm_c;
     info->scaling_scalars.b_scale = 1.0;
@@ -1235,6 +1427,12 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
     HPR_TRACE("create: lambda_Q done");
     E_ST(power_iteration(e, true, &lambda_A));
     lambda_A *= 1.05;
+    if (S.nvc || S.nrc) {
+        // reference control.cu:216-220: no noC step on cone models; a constant
+        // affine cone is meaningful even when A is zero
+        S.noC = 0;
+        if (m > 0 && lambda_A <= 0.0) lambda_A = 1.0;
+    }
     // the power iteration used pz/pq/ptmp only; iterate vectors are still zero
     e->sigma = sigma;
     e->lambda_A = lambda_A;
@@ -1268,9 +1466,45 @@ HPRQPStatus engine_create(const HPRQPModel *model, const HPRQPParams *params, En
 double engine_sigma(const Engine *e) { return e->sigma; }
 
 // ---- one step ----------------------------------------------------------------
+// one HPR step on a cone model (reference gpu_soc_iteration_step,
+// src/gpu/soc_iteration.cuh:45-83): always the full writes
+static void enqueue_soc_step(Engine *e)
+{
+    DState &S = e->S;
+    const int pg = std::max(1, std::min(e->num_sms * 8, (std::max(S.n, S.m) + kThreads - 1) / kThreads));
+    EpiSocX1 k1;
+    k1.S = S;
+    launch_rb(e, S.Q, S.w, k1);
+    k_soc_project<<<pg, kThreads, 0, e->stream>>>(S.tempv, S.x_bar, S.l, S.u, S.lin_n, S.vco, S.nvc);
+    count_launch();
+    EpiSocXFinish fx;
+    fx.S = S;
+    launch_ew(e, S.n, fx);
+    EpiTempv k2;
+    k2.S = S;
+    launch_rb(e, S.Q, S.w_bar, k2);
+    if (S.m > 0) {
+        EpiSocY1 k3;
+        k3.S = S;
+        launch_rb(e, S.A, S.tempv, k3);
+        k_soc_project<<<pg, kThreads, 0, e->stream>>>(S.pz, S.s, S.AL, S.AU, S.lin_m, S.rco, S.nrc);
+        count_launch();
+        EpiSocYFinish fy;
+        fy.S = S;
+        launch_ew(e, S.m, fy);
+    }
+    EpiW2<true> k4;
+    k4.S = S;
+    launch_rb(e, S.AT, S.y_bar, k4);
+}
+
 static void enqueue_step(Engine *e, int to_check)
 {
     DState &S = e->S;
+    if (S.nvc || S.nrc) {
+        enqueue_soc_step(e);
+        return;
+    }
     if (S.noC) {
         if (to_check) {
             EpiZXW1noC<true> k1;
@@ -1365,9 +1599,74 @@ HPRQPStatus engine_iteration_step(Engine *e, size_t inner, int to_check)
 }
 
 // ---- residuals ------------------------------------------------------------------
+// residuals of a cone model (reference gpu_soc_compute_residuals,
+// src/gpu/soc_residuals.cuh:28-77): s of the last step paired with y_bar,
+// y_bar.rhs in the dual objective, errRp from the projection of A x_bar - rhs,
+// and the distance of x_bar to its domain at every check
+static HPRQPStatus engine_residuals_soc(Engine *e, HPRQPResiduals *res)
+{
+    DState &S = e->S;
+    memset(res, 0, sizeof(*res));
+    const int pg = std::max(1, std::min(e->num_sms * 8, (std::max(S.n, S.m) + kThreads - 1) / kThreads));
+    const size_t off_q = 0, off_a = (size_t)std::max(S.Q.npart(), 1) * 7;
+    const size_t off_rp = off_a + (size_t)std::max(S.A.npart(), 1);
+    if (S.m > 0) {
+        EpiStore st;
+        st.out = S.ATdy;
+        launch_rb(e, S.AT, S.y_bar, st);
+    } else {
+        HPR_CK(cudaMemsetAsync(S.ATdy, 0, (size_t)S.n * sizeof(double), e->stream));
+    }
+    EpiResQ rq;
+    rq.S = S;
+    rq.iter0 = 0;
+    launch_rb_at(e, S.Q, S.x_bar, rq, off_q);
+    FinSpec specs[4];
+    int ns = 0;
+    specs[ns++] = spec_of<EpiResQ>(S.Q.npart(), 8, off_q);
+    if (S.m > 0) {
+        EpiSocResA ra;
+        ra.S = S;
+        launch_rb_at(e, S.A, S.x_bar, ra, off_a);
+        specs[ns++] = spec_of<EpiSocResA>(S.A.npart(), 0, off_a);
+        k_soc_project<<<pg, kThreads, 0, e->stream>>>(S.pq, S.pz, S.AL, S.AU, S.lin_m, S.rco, S.nrc);
+        count_launch();
+        EpiSocRp rp;
+        rp.S = S;
+        const int g = launch_ew(e, S.m, rp, (int)off_rp);
+        specs[ns++] = spec_of<EpiSocRp>(g, 16, off_rp);
+    }
+    const size_t off_v = off_rp + (size_t)e->num_sms * 4 * 3;
+    k_soc_project<<<pg, kThreads, 0, e->stream>>>(S.x_bar, S.ptmp, S.l, S.u, S.lin_n, S.vco, S.nvc);
+    count_launch();
+    EpiSocViol vi;
+    vi.S = S;
+    const int gv = launch_ew(e, S.n, vi, (int)off_v);
+    if (gv > 0) specs[ns++] = spec_of<EpiSocViol>(gv, 20, off_v);
+    HPRQPStatus st = finalize(e, specs, ns, true);
+    if (st) return st;
+    const double *v = e->hout->v;
+    const double max_rd = v[8], max_qx = v[9], max_aty = v[10], c_dot_x = v[11], x_dot_qx = v[12],
+                 z_dot_x = v[13];
+    const double max_ax = S.m > 0 ? v[0] : 0.0, max_rp = S.m > 0 ? v[16] : 0.0;
+    const double y_dot_s = S.m > 0 ? v[17] : 0.0, y_dot_rhs = S.m > 0 ? v[18] : 0.0;
+    const double violation = gv > 0 ? v[20] : 0.0;
+    res->primal_obj_bar = (c_dot_x + 0.5 * x_dot_qx) + e->obj_constant;
+    res->dual_obj_bar = (-0.5 * x_dot_qx + z_dot_x + y_dot_s + y_dot_rhs) + e->obj_constant;
+    res->rel_gap_bar = fabs(res->primal_obj_bar - res->dual_obj_bar) /
+                       (1.0 + fmax(fabs(res->primal_obj_bar), fabs(res->dual_obj_bar)));
+    res->err_Rd_org_bar = max_rd / (1.0 + fmax(e->norm_c_org, fmax(max_aty, max_qx)));
+    if (S.m > 0) res->err_Rp_org_bar = max_rp / (1.0 + fmax(e->norm_b_org, max_ax));
+    res->err_Rp_org_bar = fmax(res->err_Rp_org_bar, violation);
+    res->KKTx_and_gap_org_bar = fmax(res->err_Rp_org_bar, fmax(res->err_Rd_org_bar, res->rel_gap_bar));
+    res->is_updated = 1;
+    return HPRQP_STATUS_OK;
+}
+
 HPRQPStatus engine_residuals(Engine *e, HPRQPResiduals *res, size_t iter)
 {
     DState &S = e->S;
+    if (S.nvc || S.nrc) return engine_residuals_soc(e, res);
     memset(res, 0, sizeof(*res));
     const size_t off_a = 0, off_q = (size_t)std::max(S.A.npart(), 1) * 3;
     int nspec = 0;

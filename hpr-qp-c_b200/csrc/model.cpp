@@ -141,6 +141,8 @@ void model_free(HPRQPModel *model)
     model_init(model);
 }
 
+static size_t *copy_offsets(const size_t *src, size_t count);
+
 static double *copy_vec(const double *src, size_t n)
 {
     if (n == 0) return nullptr;
@@ -171,6 +173,20 @@ HPRQPStatus model_copy(HPRQPModel *dest, const HPRQPModel *src)
         return HPRQP_STATUS_ALLOCATION_FAILED;
     }
     dest->obj_constant = src->obj_constant;
+    if (src->num_var_cones) {
+        dest->var_cone_offsets = copy_offsets(src->var_cone_offsets, src->num_var_cones);
+        dest->num_var_cones = src->num_var_cones;
+    }
+    if (src->num_row_cones) {
+        dest->row_cone_offsets = copy_offsets(src->row_cone_offsets, src->num_row_cones);
+        dest->soc_rhs = copy_vec(src->soc_rhs, m);
+        dest->num_row_cones = src->num_row_cones;
+    }
+    if ((src->num_var_cones && !dest->var_cone_offsets) ||
+        (src->num_row_cones && (!dest->row_cone_offsets || !dest->soc_rhs))) {
+        model_free(dest);
+        return HPRQP_STATUS_ALLOCATION_FAILED;
+    }
     return HPRQP_STATUS_OK;
 }
 
@@ -242,9 +258,9 @@ static bool csr_indices_ok(const HPRQPMatrixCSR *m)
     return true;
 }
 
-HPRQPStatus build_from_QAbc(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c, const double *AL,
-                            const double *AU, const double *l, const double *u, double obj_constant,
-                            HPRQPModel *model)
+static HPRQPStatus build_impl(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c, const double *AL,
+                              const double *AU, const double *l, const double *u, double obj_constant,
+                              bool keep_all_rows, HPRQPModel *model)
 {
     // argument checks: src/shared/build.c:513-531, 339-379
     if (!Q || !A || !model || !c || !l || !u) return HPRQP_STATUS_INVALID_ARGUMENT;
@@ -275,7 +291,7 @@ HPRQPStatus build_from_QAbc(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, co
     for (size_t r = 0; r < m; ++r) {
         const size_t len = A->row_ptr[r + 1] - A->row_ptr[r];
         const bool free_row = std::isinf(AL[r]) && AL[r] < 0 && std::isinf(AU[r]) && AU[r] > 0;
-        if (len > 0 && !free_row) {
+        if (keep_all_rows || (len > 0 && !free_row)) {
             ++kept;
             kept_nnz += len;
         }
@@ -298,7 +314,7 @@ HPRQPStatus build_from_QAbc(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, co
     for (size_t r = 0; r < m; ++r) {
         const size_t len = A->row_ptr[r + 1] - A->row_ptr[r];
         const bool free_row = std::isinf(AL[r]) && AL[r] < 0 && std::isinf(AU[r]) && AU[r] > 0;
-        if (len == 0 || free_row) continue;
+        if (!keep_all_rows && (len == 0 || free_row)) continue;
         model->AL[row] = AL[r];
         model->AU[row] = AU[r];
         memcpy(model->A.col_ind + pos, A->col_ind + A->row_ptr[r], len * sizeof(size_t));
@@ -315,12 +331,89 @@ HPRQPStatus build_from_QAbc(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, co
     return HPRQP_STATUS_OK;
 }
 
+HPRQPStatus build_from_QAbc(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c, const double *AL,
+                            const double *AU, const double *l, const double *u, double obj_constant,
+                            HPRQPModel *model)
+{
+    return build_impl(Q, A, c, AL, AU, l, u, obj_constant, false, model);
+}
+
+// Second-order cones (reference include/shared/types.h:35-48, build.c:39-99,
+// 398): cones are contiguous suffix blocks of the variables and of the rows,
+// given by strictly increasing offsets that end at n (m); cone variables have
+// bounds (-inf, inf); on cone rows AL = -inf, AU = inf and the affine part is
+// A x - rhs in K; rhs is zero on the linear rows.  Rows are not deleted.
+static bool cone_offsets_ok(size_t count, const size_t *off, size_t length)
+{
+    if (count == 0) return true;
+    if (!off || count > length || off[0] >= length || off[count] != length) return false;
+    for (size_t k = 0; k < count; ++k)
+        if (off[k] >= off[k + 1] || off[k + 1] > length) return false;
+    return true;
+}
+
+static HPRQPStatus validate_cones(const HPRQPModel *model)
+{
+    const size_t n = model->Q.ncol, m = model->A.nrow;
+    if (!cone_offsets_ok(model->num_var_cones, model->var_cone_offsets, n) ||
+        !cone_offsets_ok(model->num_row_cones, model->row_cone_offsets, m))
+        return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (model->num_var_cones)
+        for (size_t i = model->var_cone_offsets[0]; i < n; ++i)
+            if (model->l[i] != -INFINITY || model->u[i] != INFINITY) return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (model->num_row_cones) {
+        if (!model->soc_rhs) return HPRQP_STATUS_INVALID_ARGUMENT;
+        for (size_t r = 0; r < m; ++r) {
+            if (!std::isfinite(model->soc_rhs[r])) return HPRQP_STATUS_INVALID_ARGUMENT;
+            if (r < model->row_cone_offsets[0]) {
+                if (model->soc_rhs[r] != 0.0) return HPRQP_STATUS_INVALID_ARGUMENT;
+            } else if (model->AL[r] != -INFINITY || model->AU[r] != INFINITY) {
+                return HPRQP_STATUS_INVALID_ARGUMENT;
+            }
+        }
+    }
+    return HPRQP_STATUS_OK;
+}
+
+static size_t *copy_offsets(const size_t *src, size_t count)
+{
+    size_t *d = (size_t *)malloc((count + 1) * sizeof(size_t));
+    if (d) memcpy(d, src, (count + 1) * sizeof(size_t));
+    return d;
+}
+
 HPRQPStatus build_from_QAbc_soc(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c,
                                 const double *AL, const double *AU, const double *l, const double *u,
                                 double obj_constant, const HPRQPSOCSpec *soc, HPRQPModel *model)
 {
-    if (soc && (soc->num_var_cones || soc->num_row_cones)) return HPRQP_STATUS_NOT_IMPLEMENTED;
-    return build_from_QAbc(Q, A, c, AL, AU, l, u, obj_constant, model);
+    const bool cones = soc && (soc->num_var_cones || soc->num_row_cones);
+    if (!cones) return build_from_QAbc(Q, A, c, AL, AU, l, u, obj_constant, model);
+    if (!Q || !A || !model) return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (!cone_offsets_ok(soc->num_var_cones, soc->var_offsets, Q->ncol) ||
+        !cone_offsets_ok(soc->num_row_cones, soc->row_offsets, A->nrow) || (soc->num_row_cones && !soc->rhs))
+        return HPRQP_STATUS_INVALID_ARGUMENT;
+    HPRQPStatus st = build_impl(Q, A, c, AL, AU, l, u, obj_constant, true, model);
+    if (st != HPRQP_STATUS_OK) return st;
+    if (soc->num_var_cones) {
+        model->var_cone_offsets = copy_offsets(soc->var_offsets, soc->num_var_cones);
+        if (!model->var_cone_offsets) {
+            model_free(model);
+            return HPRQP_STATUS_ALLOCATION_FAILED;
+        }
+        model->num_var_cones = soc->num_var_cones;
+    }
+    if (soc->num_row_cones) {
+        model->row_cone_offsets = copy_offsets(soc->row_offsets, soc->num_row_cones);
+        model->soc_rhs = copy_vec(soc->rhs, A->nrow);
+        if (!model->row_cone_offsets || !model->soc_rhs) {
+            model_free(model);
+            return HPRQP_STATUS_ALLOCATION_FAILED;
+        }
+        model->num_row_cones = soc->num_row_cones;
+    }
+    st = validate_cones(model);
+    if (st != HPRQP_STATUS_OK) model_free(model);
+    return st;
 }
 
 // build_from_mps lives in mps.cpp

@@ -232,7 +232,6 @@ HPRQPStatus hpr::solve_gpu_keep(const HPRQPModel *model, const HPRQPParams *para
     if (params->gram_mode < HPRQP_GRAM_OFF || params->gram_mode > HPRQP_GRAM_REQUEST)
         return HPRQP_STATUS_INVALID_ARGUMENT;
     results_init(results);
-    if (model->num_var_cones || model->num_row_cones) return HPRQP_STATUS_NOT_IMPLEMENTED;
     if (!matrix_csr_is_valid(&model->Q) || !matrix_csr_is_valid(&model->A) || !matrix_csr_is_valid(&model->AT) ||
         model->Q.ncol != model->A.ncol || !model->c || !model->l || !model->u ||
         (model->A.nrow > 0 && (!model->AL || !model->AU)))

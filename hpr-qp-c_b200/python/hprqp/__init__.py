@@ -377,6 +377,63 @@ def build_from_qabc(Q, c, A, AL, AU, l, u, obj_constant: float = 0.0) -> Model:
 build_from_QAbc = build_from_qabc
 
 
+class _SOCSpec(ctypes.Structure):
+    _fields_ = [("num_var_cones", ctypes.c_size_t), ("var_offsets", c_size_p), ("num_row_cones", ctypes.c_size_t),
+                ("row_offsets", c_size_p), ("rhs", c_double_p)]
+
+
+def build_from_qabc_soc(Q, c, A, AL, AU, l, u, var_cone_offsets=None, row_cone_offsets=None, rhs=None,
+                        obj_constant: float = 0.0) -> Model:
+    """QP with second-order cones (build_from_QAbc_soc, include/hprqp.h):
+    variables [var_cone_offsets[0], n) and rows [row_cone_offsets[0], m) are
+    split into Lorentz cones {(t, v): |v| <= t} at the offsets (count + 1
+    entries each, ending at n / m); cone variables have bounds (-inf, inf);
+    cone rows have AL = -inf, AU = inf and mean A x - rhs in K; rhs (m
+    entries) is zero on the linear rows."""
+    qn, qm, qp, qi, qv = _matrix_to_csr(Q)
+    an, am, ap, ai, av = _matrix_to_csr(A)
+    if an == 0 and am == 0:
+        am = qm
+        ap = np.zeros(1, np.uint64)
+    keep = []
+
+    def csr(nr, nc, p, i, v):
+        p = np.ascontiguousarray(p, np.uint64)
+        i = np.ascontiguousarray(i if len(i) else np.zeros(1), np.uint64)
+        v = np.ascontiguousarray(v if len(v) else np.zeros(1), np.float64)
+        keep.extend([p, i, v])
+        return _MatrixCSR(nr, nc, int(p[-1]), p.ctypes.data_as(c_size_p), i.ctypes.data_as(c_size_p),
+                          v.ctypes.data_as(c_double_p), 0)
+
+    def db(a, k, name):
+        arr = _vec(a, k, name) if k else np.zeros(1)
+        keep.append(arr)
+        return arr.ctypes.data_as(c_double_p)
+
+    def offs(o):
+        if o is None or len(o) == 0:
+            return 0, None
+        arr = np.ascontiguousarray(np.asarray(o, np.uint64))
+        keep.append(arr)
+        return len(arr) - 1, arr.ctypes.data_as(c_size_p)
+
+    nv, vp = offs(var_cone_offsets)
+    nr, rp = offs(row_cone_offsets)
+    spec = _SOCSpec(nv, vp, nr, rp, db(rhs, an, "rhs") if rhs is not None else None)
+    Qc, Ac = csr(qn, qm, qp, qi, qv), csr(an, am, ap, ai, av)
+    model = Model()
+    lib = _lib()
+    lib.build_from_QAbc_soc.argtypes = [ctypes.POINTER(_MatrixCSR), ctypes.POINTER(_MatrixCSR)] + \
+        [c_double_p] * 5 + [ctypes.c_double, ctypes.POINTER(_SOCSpec), ctypes.c_void_p]
+    lib.build_from_QAbc_soc.restype = ctypes.c_int
+    st = lib.build_from_QAbc_soc(ctypes.byref(Qc), ctypes.byref(Ac), db(c, qm, "c"),
+                                 db(AL, an, "AL") if an else None, db(AU, an, "AU") if an else None,
+                                 db(l, qm, "l"), db(u, qm, "u"), float(obj_constant), ctypes.byref(spec),
+                                 model._handle)
+    _raise_for_status(st, "build_from_QAbc_soc")
+    return model
+
+
 def build_from_instance(inst) -> Model:
     """Model from an ``instances.QPInstance`` (CSR arrays, no copies in Python)."""
     return build_from_qabc(inst.Q, inst.c, inst.A, inst.AL, inst.AU, inst.l, inst.u, inst.obj_constant)
@@ -624,6 +681,6 @@ __all__ = [
     "QPFunction", "QPLayer", "SingleQPFunction", "SolveState", "residuals", "solve_for_backward", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
     "STATUS_ALLOCATION_FAILED", "STATUS_CONTINUE", "STATUS_INVALID_ARGUMENT", "STATUS_MAX_ITER",
     "STATUS_NOT_IMPLEMENTED", "STATUS_OK", "STATUS_OPTIMAL", "STATUS_TIME_LIMIT", "build_from_mps",
-    "build_from_QAbc", "build_from_qabc", "build_from_instance", "gpu_backend_available", "optimize",
+    "build_from_QAbc", "build_from_qabc", "build_from_qabc_soc", "build_from_instance", "gpu_backend_available", "optimize",
     "read_from_mps", "status_name", "spmv", "setup_info", "model_arrays", "launch_count", "library_path",
 ]

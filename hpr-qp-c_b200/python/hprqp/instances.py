@@ -257,6 +257,74 @@ def adjoint_case(instance: int, n: int = 60, m: int = 30) -> QPInstance:
     return QPInstance(Q, A, cvec, AL, AU, l, u, 0.0, f"adjoint_{instance}")
 
 
+@dataclass
+class SOCInstance:
+    """A QP with second-order cones: the QPInstance data plus cone offsets
+    (variables [var_offsets[0], n), rows [row_offsets[0], m)) and rhs."""
+    qp: QPInstance
+    var_offsets: Optional[np.ndarray]
+    row_offsets: Optional[np.ndarray]
+    rhs: Optional[np.ndarray]
+
+
+def soc_case(instance: int, n_lin: int = 20, cone: int = 6, m_lin: int = 6, row_cone: int = 4) -> SOCInstance:
+    """min 1/2 x'Dx + c'x + t  s.t.  (t, v) in K (a variable cone), v = Bx - d,
+    random ranged rows on x, |Cx - e| <= rho (a row cone: A_K x - rhs in K),
+    x in [-1, 1]; D diagonal U(0.5, 2)."""
+    rng = np.random.default_rng(SEED_BASE + 6000 + instance)
+    k = max(cone - 1, 0)
+    n = n_lin + cone
+    x0 = rng.uniform(-0.5, 0.5, n_lin)
+    B = rng.standard_normal((k, n_lin)) * (rng.random((k, n_lin)) < 0.5)
+    d = rng.standard_normal(k)
+    G = rng.standard_normal((m_lin, n_lin)) * (rng.random((m_lin, n_lin)) < 0.4)
+    rc = max(row_cone - 1, 0)
+    C = rng.standard_normal((rc, n_lin)) * (rng.random((rc, n_lin)) < 0.5)
+    e = rng.standard_normal(rc)
+    rho = float(np.linalg.norm(C @ x0 - e)) + 0.5
+    rows, AL, AU, rhs = [], [], [], []
+    for j in range(k):  # v_j - (B x)_j = -d_j
+        r = np.zeros(n)
+        r[:n_lin] = -B[j]
+        r[n_lin + 1 + j] = 1.0
+        rows.append(r)
+        AL.append(-d[j])
+        AU.append(-d[j])
+        rhs.append(0.0)
+    gx = G @ x0
+    for j in range(m_lin):
+        r = np.zeros(n)
+        r[:n_lin] = G[j]
+        rows.append(r)
+        AL.append(gx[j] - rng.uniform(0.1, 1.0))
+        AU.append(gx[j] + rng.uniform(0.1, 1.0))
+        rhs.append(0.0)
+    m_lin_total = len(rows)
+    if row_cone:
+        rows.append(np.zeros(n))  # cone head: 0 - (-rho) = rho
+        rhs.append(-rho)
+        for j in range(rc):
+            r = np.zeros(n)
+            r[:n_lin] = C[j]
+            rows.append(r)
+            rhs.append(e[j])
+        AL += [-np.inf] * row_cone
+        AU += [np.inf] * row_cone
+    Adense = np.array(rows)
+    rr, cc = np.nonzero(Adense)
+    A = _csr_from_coo(Adense.shape[0], n, rr.astype(np.int64), cc.astype(np.int64), Adense[rr, cc])
+    qd = np.concatenate([rng.uniform(0.5, 2.0, n_lin), np.zeros(cone)])
+    nzq = np.nonzero(qd)[0]
+    Q = _csr_from_coo(n, n, nzq.astype(np.int64), nzq.astype(np.int64), qd[nzq])
+    cvec = np.concatenate([rng.standard_normal(n_lin), [1.0] if cone else [], np.zeros(k)])
+    l = np.concatenate([np.full(n_lin, -1.0), np.full(cone, -np.inf)])
+    u = np.concatenate([np.full(n_lin, 1.0), np.full(cone, np.inf)])
+    qp = QPInstance(Q, A, cvec, np.array(AL), np.array(AU), l, u, 0.0, f"soc_{instance}")
+    return SOCInstance(qp, np.array([n_lin, n], np.int64) if cone else None,
+                       np.array([m_lin_total, m_lin_total + row_cone], np.int64) if row_cone else None,
+                       np.array(rhs) if row_cone else None)
+
+
 def tiny_cases() -> List[QPInstance]:
     """Hand-written models mirroring the reference's test fixtures
     (tests/test_support.c:79-268 of the reference project): dense-list form

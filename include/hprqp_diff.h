@@ -14,6 +14,8 @@
  *
  * Everything is in the space of the model passed to the solve (the output of
  * build_from_QAbc: symmetrised Q, the kept rows of A), like HPRQPResults.
+ * Models with second-order cones are solved but not differentiated
+ * (hprqp_backward returns HPRQP_STATUS_NOT_IMPLEMENTED for them).
  */
 #ifndef HPRQP_DIFF_H
 #define HPRQP_DIFF_H

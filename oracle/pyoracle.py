@@ -432,12 +432,18 @@ def ref_gpu_lib() -> ctypes.CDLL:
     return _ref_gpu
 
 
-class RefGpuModel:
-    """A model built by the reference's own ``build_from_QAbc`` inside the
-    reference GPU library; ``solve`` runs its ``solve_gpu`` (polishing 0,
-    Gram off: the reference with ``--polishing 0 --gram off``)."""
+class _RefSOC(ctypes.Structure):
+    _fields_ = [("num_var_cones", ctypes.c_size_t), ("var_offsets", c_size_p), ("num_row_cones", ctypes.c_size_t),
+                ("row_offsets", c_size_p), ("rhs", c_double_p)]
 
-    def __init__(self, inst):
+
+class RefGpuModel:
+    """A model built by the reference's own ``build_from_QAbc`` (or
+    ``build_from_QAbc_soc`` when ``soc = (var_offsets, row_offsets, rhs)``)
+    inside the reference GPU library; ``solve`` runs its ``solve_gpu``
+    (polishing 0, Gram off: the reference with ``--polishing 0 --gram off``)."""
+
+    def __init__(self, inst, soc=None):
         L = ref_gpu_lib()
         self._keep = []
 
@@ -457,8 +463,27 @@ class RefGpuModel:
         A = csr(inst.m, inst.n, inst.A)
         self.model = _RefModel()
         L.model_init(ctypes.byref(self.model))
-        st = L.build_from_QAbc(ctypes.byref(Q), ctypes.byref(A), db(inst.c), db(inst.AL), db(inst.AU),
-                               db(inst.l), db(inst.u), float(inst.obj_constant), ctypes.byref(self.model))
+        if soc is None:
+            st = L.build_from_QAbc(ctypes.byref(Q), ctypes.byref(A), db(inst.c), db(inst.AL), db(inst.AU),
+                                   db(inst.l), db(inst.u), float(inst.obj_constant), ctypes.byref(self.model))
+        else:
+            vo, ro, rhs = soc
+
+            def offs(o):
+                if o is None:
+                    return 0, None
+                arr, p = _sz(np.asarray(o))
+                self._keep.append(arr)
+                return len(o) - 1, p
+
+            nv, vp = offs(vo)
+            nr, rp = offs(ro)
+            spec = _RefSOC(nv, vp, nr, rp, db(rhs) if rhs is not None else None)
+            L.build_from_QAbc_soc.argtypes = [ctypes.POINTER(_RefCSR), ctypes.POINTER(_RefCSR)] + [c_double_p] * 5 + \
+                [ctypes.c_double, ctypes.POINTER(_RefSOC), ctypes.POINTER(_RefModel)]
+            st = L.build_from_QAbc_soc(ctypes.byref(Q), ctypes.byref(A), db(inst.c), db(inst.AL), db(inst.AU),
+                                       db(inst.l), db(inst.u), float(inst.obj_constant), ctypes.byref(spec),
+                                       ctypes.byref(self.model))
         if st != 0:
             raise ValueError(f"reference build_from_QAbc failed: {st}")
         self.n = int(self.model.Q.ncol)
