@@ -1199,6 +1199,31 @@ __global__ void k_batch_clock(unsigned long long *t)
 
 }  // namespace hpr
 
+// std::vector storage without value-initialisation: the packing arrays are
+// fully written by the packing threads, so zero-filling gigabytes first is waste
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+    template <class U>
+    void construct(U *p) noexcept
+    {
+        ::new ((void *)p) U;
+    }
+    template <class U, class... Args>
+    void construct(U *p, Args &&...args)
+    {
+        ::new ((void *)p) U(std::forward<Args>(args)...);
+    }
+};
+template <class T>
+using HostVec = std::vector<T, NoInitAlloc<T>>;
+
 struct HPRQPBatch {
     int device = 0;
     int num_sms = 148;
@@ -1216,6 +1241,7 @@ struct HPRQPBatch {
     bool solved = false;
     // the caller's CSR index arrays of Q and A (the adjoint writes one value per caller nonzero)
     std::vector<size_t> q_rp_in, q_ci_in, a_rp_in, a_ci_in;
+    bool has_caller_csr = false;
     // adjoint buffers, allocated by the first hprqp_batch_backward
     double *adj_gx = nullptr, *adj_gy = nullptr, *adj_lx = nullptr, *adj_ly = nullptr, *adj_rel = nullptr;
     double *adj_ws = nullptr;
@@ -1290,10 +1316,11 @@ void hprqp_batch_params_set_defaults(HPRQPBatchParams *p)
     p->device_number = 0;
 }
 
-HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t *row_offsets,
-                               const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c, const double *AL,
-                               const double *AU, const double *l, const double *u, const double *obj_constants,
-                               int device_number, HPRQPBatch **out)
+static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const size_t *row_offsets,
+                                     const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c,
+                                     const double *AL, const double *AU, const double *l, const double *u,
+                                     const double *obj_constants, int device_number, bool keep_caller_csr,
+                                     HPRQPBatch **out)
 {
     using namespace hpr;
     if (!out || !var_offsets || !row_offsets || !Q || !A || !c || !l || !u || K == 0)
@@ -1313,6 +1340,10 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
     }
     if (device_number < 0 || device_number >= ndev) return HPRQP_STATUS_INVALID_ARGUMENT;
 
+    const char *trc = getenv("HPRQP_B200_BATCH_TRACE");
+    const bool ctrace = trc && trc[0] == '1';
+    auto cnow = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    const double c0 = cnow();
     HPRQPBatch *b = new HPRQPBatch();
     b->K = K;
     b->device = device_number;
@@ -1322,10 +1353,13 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
     b->models.resize(K);
     for (auto &mm : b->models) model_init(&mm);
     b->kept_rows.resize(K);
-    b->q_rp_in.assign(Q->row_ptr, Q->row_ptr + Q->nrow + 1);
-    b->q_ci_in.assign(Q->col_ind, Q->col_ind + Q->nnz);
-    b->a_rp_in.assign(A->row_ptr, A->row_ptr + A->nrow + 1);
-    b->a_ci_in.assign(A->col_ind, A->col_ind + A->nnz);
+    if (keep_caller_csr) {  // the adjoint maps gradients to the caller's nonzeros
+        b->q_rp_in.assign(Q->row_ptr, Q->row_ptr + Q->nrow + 1);
+        b->q_ci_in.assign(Q->col_ind, Q->col_ind + Q->nnz);
+        b->a_rp_in.assign(A->row_ptr, A->row_ptr + A->nrow + 1);
+        b->a_ci_in.assign(A->col_ind, A->col_ind + A->nnz);
+    }
+    b->has_caller_csr = keep_caller_csr;
     // ---- per-instance build + preprocess (the single-QP builder), threaded
     std::vector<HPRQPStatus> st_k(K, HPRQP_STATUS_OK);
     const unsigned nth = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
@@ -1373,6 +1407,7 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
             delete b;
             return st;
         }
+    const double c1 = cnow();
     // ---- pack (int32 local indices)
     size_t qnz = 0, anz = 0, qrp = 0, arp = 0, atrp = 0, nv = 0, nr = 0;
     b->inst.resize(K);
@@ -1407,12 +1442,15 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
     }
     b->total_n = nv;
     b->total_m = nr;
-    std::vector<int> h_qrp(qrp), h_arp(arp), h_atrp(atrp), h_qci(std::max<size_t>(qnz, 1)),
+    HostVec<int> h_qrp(qrp), h_arp(arp), h_atrp(atrp), h_qci(std::max<size_t>(qnz, 1)),
         h_aci(std::max<size_t>(anz, 1)), h_atci(std::max<size_t>(anz, 1));
-    std::vector<double> h_qv(std::max<size_t>(qnz, 1)), h_av(std::max<size_t>(anz, 1)), h_atv(std::max<size_t>(anz, 1)),
+    HostVec<double> h_qv(std::max<size_t>(qnz, 1)), h_av(std::max<size_t>(anz, 1)), h_atv(std::max<size_t>(anz, 1)),
         h_c(std::max<size_t>(nv, 1)), h_l(std::max<size_t>(nv, 1)), h_u(std::max<size_t>(nv, 1)),
         h_AL(std::max<size_t>(nr, 1)), h_AU(std::max<size_t>(nr, 1));
-    for (size_t k = 0; k < K; ++k) {
+    h_qci[0] = h_aci[0] = h_atci[0] = 0;
+    h_qv[0] = h_av[0] = h_atv[0] = h_c[0] = h_l[0] = h_u[0] = h_AL[0] = h_AU[0] = 0.0;
+    auto pack_worker = [&](unsigned tix) {
+    for (size_t k = tix; k < K; k += nth) {
         const HPRQPModel &M = b->models[k];
         const BInst &I = b->inst[k];
         for (size_t r = 0; r <= M.Q.nrow; ++r) h_qrp[I.q_rp + r] = (int)M.Q.row_ptr[r];
@@ -1436,6 +1474,13 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
             memcpy(&h_AU[I.row], M.AU, M.A.nrow * sizeof(double));
         }
     }
+    };
+    {
+        std::vector<std::thread> pth;
+        for (unsigned t = 0; t < nth; ++t) pth.emplace_back(pack_worker, t);
+        for (auto &t : pth) t.join();
+    }
+    const double c2 = cnow();
     // ---- device
     HPRQPStatus st = HPRQP_STATUS_OK;
     auto fail = [&](HPRQPStatus s) {
@@ -1508,8 +1553,20 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
     G.AU0 = d_AU;
     G.nmax = std::max(b->nmax, 1);
     G.mmax = std::max(b->mmax, 1);
+    if (ctrace)
+        fprintf(stderr, "[hprqp-b200 batch] create: preprocess %.3f s, pack %.3f s, device %.3f s\n", c1 - c0, c2 - c1,
+                cnow() - c2);
     *out = b;
     return HPRQP_STATUS_OK;
+}
+
+HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t *row_offsets,
+                               const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c, const double *AL,
+                               const double *AU, const double *l, const double *u, const double *obj_constants,
+                               int device_number, HPRQPBatch **out)
+{
+    return batch_create_impl(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants, device_number, true,
+                             out);
 }
 
 HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
@@ -1639,7 +1696,7 @@ HPRQPStatus hprqp_batch_backward(HPRQPBatch *b, const double *grad_x, const doub
 {
     using namespace hpr;
     if (!b || !grad_x || !out) return HPRQP_STATUS_INVALID_ARGUMENT;
-    if (!b->solved) {
+    if (!b->solved || !b->has_caller_csr) {
         fprintf(stderr, "hprqp-b200: hprqp_batch_backward needs a completed hprqp_batch_solve\n");
         return HPRQP_STATUS_INVALID_ARGUMENT;
     }
@@ -1818,13 +1875,24 @@ HPRQPStatus hprqp_solve_batch(size_t K, const size_t *var_offsets, const size_t 
                               double *residual, double *gap, double *x, double *y, double *z, double *w)
 {
     if (!params) return HPRQP_STATUS_INVALID_ARGUMENT;
+    const char *tr = getenv("HPRQP_B200_BATCH_TRACE");
+    const bool trace = tr && tr[0] == '1';
+    auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    const double t0 = now();
     HPRQPBatch *b = nullptr;
-    HPRQPStatus st = hprqp_batch_create(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants,
-                                        params->device_number, &b);
+    HPRQPStatus st = batch_create_impl(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants,
+                                       params->device_number, false, &b);
     if (st != HPRQP_STATUS_OK) return st;
+    const double t1 = now();
     st = hprqp_batch_solve(b, params);
+    const double t2 = now();
     if (st == HPRQP_STATUS_OK) st = hprqp_batch_get_results(b, status, iter, primal_obj, residual, gap, x, y, z, w);
+    const double t3 = now();
+    const double kernel_s = b->last_ms / 1e3;
     hprqp_batch_destroy(b);
+    if (trace)
+        fprintf(stderr, "[hprqp-b200 batch] create %.3f s, solve %.3f s (kernel %.3f s), results %.3f s, destroy %.3f s\n",
+                t1 - t0, t2 - t1, kernel_s, t3 - t2, now() - t3);
     return st;
 }
 
