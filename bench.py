@@ -322,6 +322,49 @@ def adjoint_leg(device: int, count: int = 256, reps: int = 3):
             "mean_minres_iters": float(g.minres_iters.mean()), "max_minres_relres": float(g.minres_relres.max())}
 
 
+def warm_start_leg(packed, base_results, device: int, reps: int = 2):
+    """Training-loop re-solve: the batch's linear costs move by 1% (c_i *
+    (1 + 0.01 N(0,1)), seeded) after a solve; the moved batch is solved cold
+    (from zero, as the reference does), warm (hprqp_batch_set_warm_start at
+    the previous solution) and warm with the previous solve's sigma.  Device time of the solve kernel and iterations of
+    each, and the largest objective difference between them."""
+    from dataclasses import replace
+
+    from hprqp import batch as hb
+
+    rng = np.random.default_rng(11)
+    moved = replace(packed, c=packed.c * (1.0 + 0.01 * rng.standard_normal(packed.c.shape[0])))
+    b = hb.Batch(moved, device_number=device)
+    cold_ms, warm_ms = [], []
+    for _ in range(reps):
+        b.set_warm_start(None)
+        cold_ms.append(b.solve(stoptol=STOPTOL))
+    cold = b.results(vectors=False)
+    b.set_warm_start(base_results.x, base_results.y, base_results.w)
+    for _ in range(reps):
+        warm_ms.append(b.solve(stoptol=STOPTOL))
+    warm = b.results(vectors=False)
+    b.set_warm_start(base_results.x, base_results.y, base_results.w, base_results.sigma)
+    ws_ms = []
+    for _ in range(reps):
+        ws_ms.append(b.solve(stoptol=STOPTOL))
+    warm_s = b.results(vectors=False)
+    b.close()
+    K = packed.K
+    cm, wm = min(cold_ms), min(warm_ms)
+    scale = np.maximum(1.0, np.abs(cold.objective))
+    return {"workload": f"{K} QPs of the batch, c moved by 1%, stoptol {STOPTOL:g}",
+            "cold": {"solves_per_s": K / (cm / 1e3), "kernel_ms": round(cm, 3), "mean_iters": float(cold.iter.mean()),
+                     "optimal": int(np.sum(cold.status == 6))},
+            "warm": {"solves_per_s": K / (wm / 1e3), "kernel_ms": round(wm, 3), "mean_iters": float(warm.iter.mean()),
+                     "optimal": int(np.sum(warm.status == 6))},
+            "warm_sigma": {"solves_per_s": K / (min(ws_ms) / 1e3), "kernel_ms": round(min(ws_ms), 3),
+                           "mean_iters": float(warm_s.iter.mean()), "optimal": int(np.sum(warm_s.status == 6))},
+            "warm_over_cold_speed": round(cm / wm, 3), "warm_sigma_over_cold_speed": round(cm / min(ws_ms), 3),
+            "max_rel_objective_diff": float(max(np.max(np.abs(warm.objective - cold.objective) / scale),
+                                                np.max(np.abs(warm_s.objective - cold.objective) / scale)))}
+
+
 def e2e_step(packed, device: int):
     """One call of hprqp_solve_batch from host buffers; returns seconds."""
     from hprqp import batch as hb
@@ -384,9 +427,10 @@ def main():
     ap.add_argument("--no-spmv", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-plain-large", action="store_true")
-    ap.add_argument("--only", choices=["spmv", "batch", "adjoint", "large", "portfolio"], default=None,
+    ap.add_argument("--no-warm", action="store_true")
+    ap.add_argument("--only", choices=["spmv", "batch", "adjoint", "large", "portfolio", "warm"], default=None,
                     help="sub-runs: only the large-QP SpMV leg, the batched solve, the adjoint, the large-QP "
-                         "plain solve or the portfolio plain solve")
+                         "plain solve, the portfolio plain solve or the warm-start re-solve")
     ap.add_argument("--spmv-reps", type=int, default=10)
     args = ap.parse_args()
 
@@ -468,7 +512,7 @@ def main():
         barrier()
         wall = time.perf_counter() - t0
     launches = hprqp.launch_count() - launches0
-    res = b.results(vectors=False)
+    res = b.results(vectors=not args.no_warm and rank == 0)
     dev_s = max_over_ranks(sum(kernel_ms) / 1e3, dist)
     wall = max_over_ranks(wall, dist)
     value = whole_job_rate(args.batch, world, args.steps, dev_s)
@@ -479,6 +523,9 @@ def main():
     if args.only == "batch":
         print(json.dumps({"value": value, "unit": "solves/s", "kernel_ms": kernel_ms, "achieved_GBs": achieved,
                           "algorithmic_bytes_per_launch": algo_bytes, "mean_iters": float(iters.mean())}), flush=True)
+        return
+    if args.only == "warm":
+        print(json.dumps({"warm_start": warm_start_leg(packed, res, local_rank)}), flush=True)
         return
 
     # end to end through the C ABI from host buffers
@@ -526,6 +573,8 @@ def main():
             line["spmv"] = spmv_leg(peak)
         if not args.no_adjoint:
             line["adjoint"] = adjoint_leg(local_rank)
+        if not args.no_warm:
+            line["warm_start"] = warm_start_leg(packed, res, local_rank)
         if not args.no_plain_large:
             line["large_qp"] = large_qp_leg(peak)
             line["portfolio"] = portfolio_leg()

@@ -87,6 +87,11 @@ struct BatchArgs {
     unsigned char *active_x;  // 1 = variable at a bound (for the adjoint)
     unsigned char *active_r;  // 1 = row at a bound
     double *col_norm_out, *row_norm_out;  // scaling of each instance (for the adjoint)
+    // optional starting point in the caller's (unscaled) variables, packed
+    // like the outputs; nullptr = start from zero as the reference does
+    const double *x_start, *w_start, *y_start;
+    const double *sigma_start;  // per instance, optional (<= 0: from the data)
+    double *sigma_out;          // per instance: sigma at the end of the solve
 };
 
 // optional per-CTA phase clocks: 0 load+scale, 1 setup norms/diag, 2 power
@@ -466,6 +471,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             if (tid == 0) {
                 const double nb = sqrt(v[0]), nc = sqrt(v[1]);
                 S.sigma = (nb > 1e-16 && nc > 1e-16 && nb < 1e16 && nc < 1e16) ? nb / nc : 1.0;
+                if (B.sigma_start && B.sigma_start[k] > 0.0) S.sigma = clampd(B.sigma_start[k], 1e-12, 1e12);
                 S.noC = n > 0 && 5.0 * v[2] > 4.0 * (double)n;
                 S.q_is_diag = v[3] <= 1e-15;
                 S.lQ = S.q_is_diag ? v2[0] : 0.0;
@@ -486,12 +492,19 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
         }
         __syncthreads();
         PHASE_ADD(2);
-        // zero iterates; diagonal factors
+        // starting iterates (zero, or the warm start scaled into the solver's
+        // variables: x_s = x * col_norm, y_s = y * row_norm, the inverse of
+        // the output map below; the Halpern anchors start at the same point);
+        // diagonal factors
+        const bool warm = B.x_start != nullptr;
         for (int i = tid; i < n; i += kBT) {
-            V.x[i] = V.x_bar[i] = V.x_hat[i] = V.w[i] = V.w_bar[i] = 0.0;
+            const double xs = warm ? B.x_start[I.var + i] * V.col_norm[i] : 0.0;
+            const double ws = warm ? B.w_start[I.var + i] * V.col_norm[i] : 0.0;
+            V.x[i] = V.x_bar[i] = V.x_hat[i] = V.last_x[i] = xs;
+            V.w[i] = V.w_bar[i] = V.last_w[i] = ws;
             V.ATy[i] = V.ATy_bar[i] = V.ATdy[i] = V.Qw[i] = V.Qw_bar[i] = V.Qx[i] = 0.0;
             V.dQw[i] = V.QATdy[i] = V.dx[i] = V.dw[i] = V.z_bar[i] = V.tempv[i] = 0.0;
-            V.last_x[i] = V.last_Qw[i] = V.last_w[i] = V.last_ATy[i] = 0.0;
+            V.last_Qw[i] = V.last_ATy[i] = 0.0;
             if (S.q_is_diag) {
                 const double inv = 1.0 / (1.0 + S.sigma * V.diag_Q[i]);
                 V.fact2[i] = inv;
@@ -500,7 +513,18 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
                 V.fact_M[i] = S.sigma * S.sigma * inv;
             }
         }
-        for (int i = tid; i < m; i += kBT) V.y[i] = V.y_bar[i] = V.Ax[i] = V.dy[i] = V.s[i] = V.last_y[i] = 0.0;
+        for (int i = tid; i < m; i += kBT) {
+            V.y[i] = V.y_bar[i] = V.last_y[i] = warm ? B.y_start[I.row + i] * V.row_norm[i] : 0.0;
+            V.Ax[i] = V.dy[i] = V.s[i] = 0.0;
+        }
+        __syncthreads();
+        if (warm) {
+            // the products the step carries with the iterates: A'y, and Q w
+            // on the noC path (reference iteration.cu:831-920)
+            if (m > 0)
+                cta_spmv(AT, V.y, scratch, [&](int i, double s) { V.ATy[i] = V.ATy_bar[i] = V.last_ATy[i] = s; });
+            if (S.noC) cta_spmv(Q, V.w, scratch, [&](int i, double s) { V.Qw[i] = V.Qw_bar[i] = V.last_Qw[i] = s; });
+        }
         if (tid == 0) {
             S.restart_flag = 0;
             S.first_restart = 1;
@@ -898,7 +922,10 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             if (tid == 0) {
                 const double el = S.scal[1];
                 int fs;
-                if (S.kkt < B.stoptol) fs = 6;
+                // a warm start is not an HPR iterate: its y and z need not lie
+                // in the normal cones the residual formulas assume, so it is
+                // not accepted as optimal before the first step
+                if (S.kkt < B.stoptol && !(warm && iter == 0)) fs = 6;
                 else if (iter == B.max_iter) fs = 4;
                 else if (el > B.time_limit) fs = 5;
                 else fs = 7;
@@ -987,6 +1014,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             B.resid[k] = S.kkt;
             B.gap[k] = S.gap;
             B.restarts[k] = (int)S.times;
+            B.sigma_out[k] = S.sigma;
         }
         __syncthreads();
     }
@@ -1248,6 +1276,10 @@ struct HPRQPBatch {
     int *adj_it = nullptr, *adj_counter = nullptr;
     size_t adj_ws_count = 0;
     double last_adjoint_ms = 0.0;
+    // warm start (device packing: total variables, kept rows), set by
+    // hprqp_batch_set_warm_start
+    double *start_x = nullptr, *start_w = nullptr, *start_y = nullptr, *start_sigma = nullptr;
+    unsigned long long *d_t0 = nullptr, *d_phase = nullptr;
     // host copies of the preprocessed models (kept for the adjoint)
     std::vector<HPRQPModel> models;
 };
@@ -1510,7 +1542,8 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         (st = balloc(b, &G.x, h_c.size())) || (st = balloc(b, &G.z, h_c.size())) || (st = balloc(b, &G.w, h_c.size())) ||
         (st = balloc(b, &G.y, h_AL.size())) || (st = balloc(b, &G.status, K)) || (st = balloc(b, &G.iters, K)) ||
         (st = balloc(b, &G.pobj, K)) || (st = balloc(b, &G.resid, K)) || (st = balloc(b, &G.gap, K)) ||
-        (st = balloc(b, &G.restarts, K)) || (st = balloc(b, &G.active_x, h_c.size())) ||
+        (st = balloc(b, &G.restarts, K)) || (st = balloc(b, &G.sigma_out, K)) ||
+        (st = balloc(b, &G.active_x, h_c.size())) ||
         (st = balloc(b, &G.active_r, h_AL.size())) || (st = balloc(b, &G.col_norm_out, h_c.size())) ||
         (st = balloc(b, &G.row_norm_out, h_AL.size())))
         return fail(st);
@@ -1598,9 +1631,11 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     G.check_iter = (int)p->check_iter;
     G.print_frequency = p->print_frequency;
     G.use_scaling = p->use_scaling;
-    unsigned long long *d_t0 = nullptr;
-    HPRQPStatus st = balloc(b, &d_t0, 1);
-    if (st) return st;
+    if (!b->d_t0) {
+        HPRQPStatus st = balloc(b, &b->d_t0, 1);
+        if (st) return st;
+    }
+    unsigned long long *d_t0 = b->d_t0;
     B_CK(cudaMemsetAsync(G.counter, 0, sizeof(int), b->stream));
     k_batch_clock<<<1, 1, 0, b->stream>>>(d_t0);
     count_launch();
@@ -1615,8 +1650,11 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     const char *pe = getenv("HPRQP_B200_BATCH_PHASES");
     unsigned long long *d_phase = nullptr;
     if (pe && pe[0] == '1') {
-        HPRQPStatus st2 = balloc(b, &d_phase, (size_t)grid * 8);
-        if (st2) return st2;
+        if (!b->d_phase) {
+            HPRQPStatus st2 = balloc(b, &b->d_phase, (size_t)grid * 8);
+            if (st2) return st2;
+        }
+        d_phase = b->d_phase;
         B_CK(cudaMemsetAsync(d_phase, 0, (size_t)grid * 8 * sizeof(unsigned long long), b->stream));
     }
     G.phase_clk = d_phase;
@@ -1643,6 +1681,63 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
                 100 * tot[0] / tot[7], 100 * tot[1] / tot[7], 100 * tot[2] / tot[7], 100 * tot[3] / tot[7],
                 100 * tot[4] / tot[7], 100 * tot[5] / tot[7], 100 * tot[6] / tot[7], grid, smem);
     }
+    return HPRQP_STATUS_OK;
+}
+
+HPRQPStatus hprqp_batch_set_warm_start(HPRQPBatch *b, const double *x0, const double *y0, const double *w0,
+                                       const double *sigma0)
+{
+    using namespace hpr;
+    if (!b) return HPRQP_STATUS_INVALID_ARGUMENT;
+    BatchArgs &G = b->args;
+    if (!x0) {
+        G.x_start = G.w_start = G.y_start = G.sigma_start = nullptr;
+        return HPRQP_STATUS_OK;
+    }
+    if (sigma0)
+        for (size_t k = 0; k < b->K; ++k)
+            if (std::isnan(sigma0[k]) || std::isinf(sigma0[k])) return HPRQP_STATUS_INVALID_ARGUMENT;
+    const size_t N = b->total_n, M = b->total_m;
+    for (size_t i = 0; i < N; ++i)
+        if (!std::isfinite(x0[i]) || (w0 && !std::isfinite(w0[i]))) return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (y0)
+        for (size_t i = 0; i < b->total_m_orig; ++i)
+            if (!std::isfinite(y0[i])) return HPRQP_STATUS_INVALID_ARGUMENT;
+    B_CK(cudaSetDevice(b->device));
+    HPRQPStatus st;
+    if (!b->start_x &&
+        ((st = balloc(b, &b->start_x, N)) || (st = balloc(b, &b->start_w, N)) || (st = balloc(b, &b->start_y, M)) ||
+         (st = balloc(b, &b->start_sigma, b->K))))
+        return st;
+    // y0 is given on the caller's rows: keep the rows the builder kept
+    std::vector<double> hy(std::max<size_t>(M, 1), 0.0);
+    if (y0)
+        for (size_t k = 0; k < b->K; ++k) {
+            const auto &kr = b->kept_rows[k];
+            for (size_t r = 0; r < kr.size(); ++r) hy[b->inst[k].row + r] = y0[b->row_off[k] + kr[r]];
+        }
+    if (N) {
+        B_CK(cudaMemcpyAsync(b->start_x, x0, N * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+        B_CK(cudaMemcpyAsync(b->start_w, w0 ? w0 : x0, N * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    }
+    if (M) B_CK(cudaMemcpyAsync(b->start_y, hy.data(), M * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    if (sigma0)
+        B_CK(cudaMemcpyAsync(b->start_sigma, sigma0, b->K * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    B_CK(cudaStreamSynchronize(b->stream));
+    G.x_start = b->start_x;
+    G.w_start = b->start_w;
+    G.y_start = b->start_y;
+    G.sigma_start = sigma0 ? b->start_sigma : nullptr;
+    return HPRQP_STATUS_OK;
+}
+
+HPRQPStatus hprqp_batch_get_sigma(const HPRQPBatch *b, double *sigma)
+{
+    if (!b || !b->solved || !sigma) return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (cudaMemcpyAsync(sigma, b->args.sigma_out, b->K * sizeof(double), cudaMemcpyDeviceToHost, b->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
     return HPRQP_STATUS_OK;
 }
 

@@ -37,6 +37,8 @@ def _configure():
                                        ctypes.POINTER(_MatrixCSR), c_double_p, c_double_p, c_double_p, c_double_p,
                                        c_double_p, c_double_p, ctypes.c_int, ctypes.POINTER(vp)]
     lib.hprqp_batch_solve.argtypes = [vp, ctypes.POINTER(BatchParams)]
+    lib.hprqp_batch_set_warm_start.argtypes = [vp, c_double_p, c_double_p, c_double_p, c_double_p]
+    lib.hprqp_batch_get_sigma.argtypes = [vp, c_double_p]
     lib.hprqp_batch_last_solve_ms.argtypes = [vp]
     lib.hprqp_batch_last_solve_ms.restype = ctypes.c_double
     lib.hprqp_batch_get_results.argtypes = [vp, ctypes.POINTER(ctypes.c_int), c_size_p, c_double_p, c_double_p,
@@ -137,6 +139,7 @@ class BatchResult:
     z: np.ndarray
     w: np.ndarray
     solve_ms: float
+    sigma: Optional[np.ndarray] = None  # per instance, at the end of the solve
 
 
 @dataclass
@@ -184,6 +187,32 @@ class Batch:
         self._handle = handle
         self.n, self.m, self.K = n, m, p.K
 
+    def set_warm_start(self, x0=None, y0=None, w0=None, sigma0=None):
+        """Start the following solves at (x0, y0, w0) -- e.g. the x, y, w of
+        a solve of a nearby batch -- instead of zero, optionally with that
+        solve's per-instance sigma (:attr:`BatchResult.sigma`); ``x0=None``
+        clears it (hprqp_batch_set_warm_start)."""
+        if x0 is None:
+            _raise_for_status(_lib().hprqp_batch_set_warm_start(self._handle, None, None, None, None),
+                              "hprqp_batch_set_warm_start")
+            return
+
+        def vec(a, size, name):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, np.float64).reshape(-1)
+            if a.shape[0] != size:
+                raise ValueError(f"warm start {name}: expected {size} entries, got {a.shape[0]}")
+            return a if size else np.zeros(1)
+
+        x = vec(x0, self.n, "x0")
+        y = vec(y0, self.m, "y0")
+        w = vec(w0, self.n, "w0")
+        sg = vec(sigma0, self.K, "sigma0")
+        ptr = (lambda a: None if a is None else a.ctypes.data_as(c_double_p))
+        _raise_for_status(_lib().hprqp_batch_set_warm_start(self._handle, ptr(x), ptr(y), ptr(w), ptr(sg)),
+                          "hprqp_batch_set_warm_start")
+
     def solve(self, **kw) -> float:
         params = default_params(**kw)
         _raise_for_status(_lib().hprqp_batch_solve(self._handle, ctypes.byref(params)), "hprqp_batch_solve")
@@ -206,8 +235,11 @@ class Batch:
                                             res.ctypes.data_as(c_double_p), gap.ctypes.data_as(c_double_p),
                                             vec(x), vec(y), vec(z), vec(w))
         _raise_for_status(st, "hprqp_batch_get_results")
+        sigma = np.zeros(K)
+        _raise_for_status(_lib().hprqp_batch_get_sigma(self._handle, sigma.ctypes.data_as(c_double_p)),
+                          "hprqp_batch_get_sigma")
         return BatchResult(status, it.astype(np.int64), obj, res, gap, x[:self.n], y[:self.m], z[:self.n],
-                           w[:self.n], float(_lib().hprqp_batch_last_solve_ms(self._handle)))
+                           w[:self.n], float(_lib().hprqp_batch_last_solve_ms(self._handle)), sigma)
 
     def backward(self, grad_x, grad_y=None, tol: float = 1e-12) -> Gradients:
         """Implicit-differentiation adjoint of the last solve (one MINRES

@@ -46,13 +46,19 @@ class QPFunction(torch.autograd.Function):
         packed = replace(structure, q_data=_np(q_data), a_data=_np(a_data), c=_np(c), AL=_np(AL), AU=_np(AU),
                          l=_np(l), u=_np(u))
         kw = dict(solve_kw)
+        start = kw.pop("warm_start", None)
+        store = kw.pop("_warm_store", None)
         batch = Batch(packed, device_number=kw.pop("device_number", 0))
         try:
+            if start is not None:
+                batch.set_warm_start(*start)
             batch.solve(**kw)
             res = batch.results()
         except Exception:
             batch.close()
             raise
+        if store is not None:
+            store["point"] = (res.x.copy(), res.y.copy(), res.w.copy(), res.sigma.copy())
         ctx.batch = batch
         ctx.backward_tol = backward_tol
         ctx.device = c.device
@@ -148,13 +154,22 @@ class QPLayer(torch.nn.Module):
     arrays of Q and A (its numeric arrays are ignored); ``forward`` takes the
     data tensors packed the same way and returns ``(x, y)``.  Solver
     parameters (``stoptol``, default 1e-8, ``max_iter``, ...) are passed as
-    keywords."""
+    keywords.  With ``warm_start=True`` every forward after the first starts
+    the solver at the previous forward's solution and sigma
+    (hprqp_batch_set_warm_start):
+    in a training loop the data move a little per step, so the new solution
+    is near the old one.  The gradients do not depend on the starting point."""
 
-    def __init__(self, structure: Packed, backward_tol: float = 1e-12, **solve_kw):
+    def __init__(self, structure: Packed, backward_tol: float = 1e-12, warm_start: bool = False, **solve_kw):
         super().__init__()
         self.structure = structure
         self.backward_tol = backward_tol
+        self.warm_start = warm_start
         self.solve_kw = {"stoptol": 1e-8, **solve_kw}
+        self._warm = {}  # (x, y, w, sigma) of the last forward
 
     def forward(self, q_data, a_data, c, AL, AU, l, u):
-        return QPFunction.apply(self.structure, self.solve_kw, self.backward_tol, q_data, a_data, c, AL, AU, l, u)
+        kw = self.solve_kw
+        if self.warm_start:
+            kw = {**kw, "warm_start": self._warm.get("point"), "_warm_store": self._warm}
+        return QPFunction.apply(self.structure, kw, self.backward_tol, q_data, a_data, c, AL, AU, l, u)

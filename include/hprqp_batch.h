@@ -47,8 +47,29 @@ HPRQPStatus hprqp_batch_create(size_t num_instances, const size_t *var_offsets, 
                                const double *obj_constants, int device_number, HPRQPBatch **out);
 
 /* Solve all instances (one persistent kernel; inputs already on the device).
- * May be called repeatedly; every call starts from the original data. */
+ * May be called repeatedly; every call starts from the original data, at
+ * zero or at the point set by hprqp_batch_set_warm_start. */
 HPRQPStatus hprqp_batch_solve(HPRQPBatch *batch, const HPRQPBatchParams *params);
+
+/* Start the following hprqp_batch_solve calls from a given point instead of
+ * zero (an addition: the reference always starts from zero, its iterates
+ * being zero-filled at allocation, reference src/gpu/context.cu:75-96).
+ * x0 and w0: total variables; y0: the caller's total rows (rows removed by
+ * preprocessing are ignored).  w0 == NULL uses x0, y0 == NULL uses zero;
+ * x0 == NULL clears the warm start.  The typical point is the x, y, w of a
+ * solve of a nearby batch (hprqp_batch_get_results), e.g. the previous step
+ * of a training loop.  Each instance starts its iterates and Halpern anchors
+ * there (scaled like the data); the point is never accepted as optimal
+ * before the first step.  sigma0 (one per instance, or NULL): the starting
+ * step-size ratio sigma, e.g. hprqp_batch_get_sigma of that solve; entries
+ * <= 0, and NULL, keep the reference's data-based sigma0 (reference
+ * src/gpu/control.cu:196-200).  Non-finite entries:
+ * HPRQP_STATUS_INVALID_ARGUMENT.  The values are copied. */
+HPRQPStatus hprqp_batch_set_warm_start(HPRQPBatch *batch, const double *x0, const double *y0, const double *w0,
+                                       const double *sigma0);
+
+/* sigma of each instance at the end of the last hprqp_batch_solve. */
+HPRQPStatus hprqp_batch_get_sigma(const HPRQPBatch *batch, double *sigma);
 
 /* Device time of the last hprqp_batch_solve kernel, milliseconds. */
 double hprqp_batch_last_solve_ms(const HPRQPBatch *batch);
