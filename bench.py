@@ -216,7 +216,8 @@ def cpu_reference_rate(ids, cores: int):
 
 
 def spmv_leg(peak_gbs: float, reps: int = 10):
-    """Row-tiled SpMV on the large power-law QP's A and Q (device timing)."""
+    """Row-tiled SpMV on the large power-law QP's A and Q (device timing),
+    beside the gather bound of the same matrix (hprqp_b200_gather_bound)."""
     import hprqp
     from hprqp import instances
 
@@ -228,12 +229,20 @@ def spmv_leg(peak_gbs: float, reps: int = 10):
         "Q": (inst.Q.indptr, inst.Q.indices, inst.Q.data, inst.n, inst.n),
     }.items():
         x = rng.standard_normal(ncol)
-        _, ms = hprqp.spmv(ip, ii, dd, ncol, x, reps=reps)
+        y, ms = hprqp.spmv(ip, ii, dd, ncol, x, reps=reps)
+        total, bound_ms = hprqp.gather_bound(ip, ii, dd, ncol, x, reps=reps)
+        if abs(total - float(np.sum(y))) > 1e-9 * max(1.0, float(np.sum(np.abs(y)))):
+            raise RuntimeError(f"gather bound checksum {total} != sum(M x) {np.sum(y)}")
         nnz = int(ip[-1])
         algo = 12 * nnz + 4 * (nrow + 1) + 8 * ncol + 8 * nrow
         gbs = algo / (ms * 1e-3) / 1e9
         out[name] = {"nnz": nnz, "ms": round(ms, 4), "GB/s": round(gbs, 1), "frac": round(gbs / peak_gbs, 4),
-                     "bytes": algo}
+                     "bytes": algo,
+                     # the same bytes over the time of a pass with no row structure at all:
+                     # what any CSR kernel can reach on this column pattern
+                     "gather_bound": {"ms": round(bound_ms, 4), "GB/s": round(algo / (bound_ms * 1e-3) / 1e9, 1),
+                                      "frac": round(algo / (bound_ms * 1e-3) / 1e9 / peak_gbs, 4),
+                                      "spmv_over_bound": round(bound_ms / ms, 4)}}
     return out
 
 

@@ -155,6 +155,9 @@ class _Library:
             getattr(lib, f"hprqp_results_{name}_data").restype = c_double_p
         lib.hprqp_b200_spmv.argtypes = [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, c_size_p, c_size_p,
                                         c_double_p, c_double_p, c_double_p, ctypes.c_int, c_double_p]
+        lib.hprqp_b200_gather_bound.argtypes = [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, c_size_p,
+                                                c_size_p, c_double_p, c_double_p, ctypes.c_int, c_double_p,
+                                                c_double_p]
         lib.hprqp_b200_setup.argtypes = [ctypes.POINTER(_ModelStruct), ctypes.POINTER(_ParamsStruct)] + \
             [c_double_p] * 11
         lib.hprqp_b200_launch_count.restype = ctypes.c_uint64
@@ -612,6 +615,23 @@ def spmv(indptr, indices, data, ncol: int, x, reps: int = 1):
                                 int(reps), ctypes.byref(ms))
     _raise_for_status(st, "hprqp_b200_spmv")
     return y[:nrow], ms.value
+
+
+def gather_bound(indptr, indices, data, ncol: int, x, reps: int = 1):
+    """The floor of any CSR product with this sparsity pattern
+    (hprqp_b200_gather_bound): every index and value streamed and every
+    x[col] gathered, no row structure.  Returns (sum of all products,
+    mean_ms_per_pass)."""
+    ip, ipp = _ptr_sz(np.asarray(indptr))
+    ii, iip = _ptr_sz(np.asarray(indices))
+    dd, ddp = _ptr_db(np.asarray(data))
+    xx, xxp = _ptr_db(np.asarray(x, dtype=np.float64))
+    ms = ctypes.c_double(0.0)
+    total = ctypes.c_double(0.0)
+    st = _lib().hprqp_b200_gather_bound(len(indptr) - 1, int(ncol), int(indptr[-1]), ipp, iip, ddp, xxp, int(reps),
+                                        ctypes.byref(ms), ctypes.byref(total))
+    _raise_for_status(st, "hprqp_b200_gather_bound")
+    return total.value, ms.value
 
 
 def setup_info(model: Model, params: Optional[Parameters] = None, dump: bool = False):

@@ -29,6 +29,18 @@ HPRQPStatus hprqp_b200_spmv(size_t nrow, size_t ncol, size_t nnz, const size_t *
                             const size_t *col_ind, const double *values, const double *x, double *y,
                             int reps, double *ms_per_spmv);
 
+/* The floor of any CSR product with this matrix's sparsity pattern (an
+ * addition, a yardstick for hprqp_b200_spmv): one kernel streams every
+ * column index and value once and gathers every x[col], with no row
+ * structure (each warp takes 2048 consecutive entries).  Timed like
+ * hprqp_b200_spmv (one untimed pass, then `reps` timed passes, the same L2
+ * eviction rule); *ms_per_pass = mean device time of one pass, *checksum =
+ * the sum of all products v[k] * x[col[k]] (the sum of the entries of M x,
+ * up to rounding). */
+HPRQPStatus hprqp_b200_gather_bound(size_t nrow, size_t ncol, size_t nnz, const size_t *row_ptr,
+                                    const size_t *col_ind, const double *values, const double *x, int reps,
+                                    double *ms_per_pass, double *checksum);
+
 /* The solver's residual kernels at a caller-given point (x, y, z) in the
  * original space of the preprocessed model (x, z: n entries, y: m): setup as
  * solve_gpu performs it, then the fused residual SpMVs and reductions

@@ -64,6 +64,33 @@ def test_spmv_zipf_rows(engine_lib):
     _spmv_check(engine_lib, indptr, indices, data, 4000, 4)
 
 
+def test_spmv_contiguous_runs(engine_lib):
+    """rows made of consecutive columns (dense blocks) run the staged tile
+    kernel; ragged lengths, empty rows and a row longer than a tile"""
+    rng = np.random.default_rng(7)
+    ncol = 3000
+    lens = np.concatenate([rng.integers(1, 300, 500), [1500, 2999], np.zeros(5, int), np.ones(40, int)])
+    rng.shuffle(lens)
+    indptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    indices = np.concatenate([np.arange(s, s + l) for s, l in
+                              zip((rng.integers(0, ncol - l + 1) for l in lens), lens)]).astype(np.int64)
+    data = rng.standard_normal(int(indptr[-1]))
+    _spmv_check(engine_lib, indptr, indices, data, ncol, 8)
+
+
+def test_gather_bound_checksum(engine_lib):
+    """hprqp_b200_gather_bound does the whole pass: its sum of products is
+    the sum of the entries of M x"""
+    rng = np.random.default_rng(9)
+    lens = np.minimum(rng.zipf(1.6, 30000), 2500)
+    indptr, indices, data = _csr_from_lengths(rng, lens, 6000)
+    x = rng.standard_normal(6000)
+    y, _ = engine_lib.spmv(indptr, indices, data, 6000, x)
+    total, ms = engine_lib.gather_bound(indptr, indices, data, 6000, x, reps=3)
+    assert ms > 0
+    assert abs(total - float(np.sum(y))) <= 1e-12 * float(np.sum(np.abs(data * x[indices])))
+
+
 def test_spmv_empty_matrix(engine_lib):
     indptr = np.zeros(11, np.int64)
     y, _ = engine_lib.spmv(indptr, np.zeros(0, np.int64), np.zeros(0), 5, np.ones(5))
