@@ -41,11 +41,12 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "hpr-qp-c_b200" / "python"))
 sys.path.insert(0, str(ROOT / "oracle"))
 
-# DRAM bytes moved per algorithmic byte by k_batch_solve: ncu on a 148-QP
-# launch of this workload read+wrote 41.152 GB (dram__bytes_read.sum +
-# dram__bytes_write.sum) for 231.757 GB of algorithmic bytes; each
-# instance's matrices stay in L2 across its iterations.
-BATCH_DRAM_PER_ALGO_BYTE = 41.152e9 / 231.757e9
+# DRAM bytes moved per algorithmic byte by k_batch_solve: ncu on a 296-QP
+# launch of this workload (two 512-thread CTAs per SM, one instance each)
+# read+wrote 373.270 GB (dram__bytes_read.sum + dram__bytes_write.sum) for
+# 504.759 GB of algorithmic bytes; the 296 concurrent instances' matrices
+# and vectors no longer all fit in L2, so part of each iteration re-reads HBM.
+BATCH_DRAM_PER_ALGO_BYTE = 373.270e9 / 504.759e9
 METRIC = "solves/s to 1e-6 rel-KKT, batched vs plain on 1 B200; SpMV GB/s vs HBM peak"
 STOPTOL = 1e-6
 BATCH = 4096
@@ -560,7 +561,7 @@ def main():
                     "optimal": e2e_ok},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": algo_bytes * BATCH_DRAM_PER_ALGO_BYTE,
-                         "traffic_source": "ncu DRAM bytes of a 148-QP launch of this workload, scaled by "
+                         "traffic_source": "ncu DRAM bytes of a 296-QP launch of this workload, scaled by "
                                            "algorithmic bytes (instance-iterations)",
                          "kernel": "k_batch_solve",
                          "algorithmic_bytes_per_launch": algo_bytes, "peak_kind": peak_kind},
