@@ -99,6 +99,7 @@ struct BatchArgs {
     const double *x_start, *w_start, *y_start;
     const double *sigma_start;  // per instance, optional (<= 0: from the data)
     double *sigma_out;          // per instance: sigma at the end of the solve
+    double *seconds_out;        // per instance: device time from its start to its end on its CTA
 };
 
 // optional per-CTA phase clocks: 0 load+scale, 1 setup norms/diag, 2 power
@@ -361,6 +362,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
         const int k = s_inst;
         __syncthreads();
         if (k < 0) break;
+        const unsigned long long inst_t0 = globaltimer_ns();
         const BInst I = B.inst[k];
         const int n = I.n, m = I.m;
         LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz};
@@ -1022,6 +1024,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             B.gap[k] = S.gap;
             B.restarts[k] = (int)S.times;
             B.sigma_out[k] = S.sigma;
+            B.seconds_out[k] = 1e-9 * (double)(globaltimer_ns() - inst_t0);
         }
         __syncthreads();
     }
@@ -1550,6 +1553,7 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         (st = balloc(b, &G.y, h_AL.size())) || (st = balloc(b, &G.status, K)) || (st = balloc(b, &G.iters, K)) ||
         (st = balloc(b, &G.pobj, K)) || (st = balloc(b, &G.resid, K)) || (st = balloc(b, &G.gap, K)) ||
         (st = balloc(b, &G.restarts, K)) || (st = balloc(b, &G.sigma_out, K)) ||
+        (st = balloc(b, &G.seconds_out, K)) ||
         (st = balloc(b, &G.active_x, h_c.size())) ||
         (st = balloc(b, &G.active_r, h_AL.size())) || (st = balloc(b, &G.col_norm_out, h_c.size())) ||
         (st = balloc(b, &G.row_norm_out, h_AL.size())))
@@ -1738,14 +1742,24 @@ HPRQPStatus hprqp_batch_set_warm_start(HPRQPBatch *b, const double *x0, const do
     return HPRQP_STATUS_OK;
 }
 
-HPRQPStatus hprqp_batch_get_sigma(const HPRQPBatch *b, double *sigma)
+// copy K doubles of a per-instance output of the last solve to the host
+static HPRQPStatus batch_download(const HPRQPBatch *b, const double *d, double *h)
 {
-    if (!b || !b->solved || !sigma) return HPRQP_STATUS_INVALID_ARGUMENT;
-    if (cudaMemcpyAsync(sigma, b->args.sigma_out, b->K * sizeof(double), cudaMemcpyDeviceToHost, b->stream) !=
-            cudaSuccess ||
+    if (!b || !b->solved || !h) return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (cudaMemcpyAsync(h, d, b->K * sizeof(double), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess ||
         cudaStreamSynchronize(b->stream) != cudaSuccess)
         return HPRQP_STATUS_NOT_IMPLEMENTED;
     return HPRQP_STATUS_OK;
+}
+
+HPRQPStatus hprqp_batch_get_sigma(const HPRQPBatch *b, double *sigma)
+{
+    return batch_download(b, b ? b->args.sigma_out : nullptr, sigma);
+}
+
+HPRQPStatus hprqp_batch_get_times(const HPRQPBatch *b, double *seconds)
+{
+    return batch_download(b, b ? b->args.seconds_out : nullptr, seconds);
 }
 
 double hprqp_batch_last_solve_ms(const HPRQPBatch *b) { return b ? b->last_ms : 0.0; }

@@ -226,6 +226,29 @@ class Model:
         # the binding model struct starts with an HPRQPModel
         return ctypes.cast(self._handle, ctypes.POINTER(_ModelStruct)).contents
 
+    def to_instance(self, name: str = ""):
+        """Copies of the built (preprocessed) model's arrays as a
+        :class:`hprqp.instances.QPInstance` -- Q, A, c, AL, AU, l, u and the
+        objective constant -- e.g. to solve models read from MPS files as one
+        batch (:mod:`hprqp.batch`).  Cone models are not supported."""
+        from .instances import CSR, QPInstance
+
+        st = self._struct()
+        if st.num_var_cones or st.num_row_cones:
+            raise ValueError("to_instance: cone models are not supported")
+
+        def csr(M):
+            nrow, nnz = int(M.nrow), int(M.nnz)
+            ip = np.ctypeslib.as_array(M.row_ptr, (nrow + 1,)).astype(np.int64)
+            ii = np.ctypeslib.as_array(M.col_ind, (nnz,)).astype(np.int64) if nnz else np.zeros(0, np.int64)
+            dd = np.ctypeslib.as_array(M.values, (nnz,)).copy() if nnz else np.zeros(0)
+            return CSR(nrow, int(M.ncol), ip, ii, dd)
+
+        n, m = int(st.Q.nrow), int(st.A.nrow)
+        vec = (lambda p, k: np.ctypeslib.as_array(p, (k,)).copy() if k else np.zeros(0))  # noqa: E731
+        return QPInstance(csr(st.Q), csr(st.A), vec(st.c, n), vec(st.AL, m), vec(st.AU, m), vec(st.l, n),
+                          vec(st.u, n), float(st.obj_constant), name)
+
 
 class Parameters:
     def __init__(self, **kwargs) -> None:

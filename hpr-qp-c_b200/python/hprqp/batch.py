@@ -39,6 +39,7 @@ def _configure():
     lib.hprqp_batch_solve.argtypes = [vp, ctypes.POINTER(BatchParams)]
     lib.hprqp_batch_set_warm_start.argtypes = [vp, c_double_p, c_double_p, c_double_p, c_double_p]
     lib.hprqp_batch_get_sigma.argtypes = [vp, c_double_p]
+    lib.hprqp_batch_get_times.argtypes = [vp, c_double_p]
     lib.hprqp_batch_last_solve_ms.argtypes = [vp]
     lib.hprqp_batch_last_solve_ms.restype = ctypes.c_double
     lib.hprqp_batch_get_results.argtypes = [vp, ctypes.POINTER(ctypes.c_int), c_size_p, c_double_p, c_double_p,
@@ -140,6 +141,7 @@ class BatchResult:
     w: np.ndarray
     solve_ms: float
     sigma: Optional[np.ndarray] = None  # per instance, at the end of the solve
+    seconds: Optional[np.ndarray] = None  # per instance, its own time on its CTA
 
 
 @dataclass
@@ -238,8 +240,11 @@ class Batch:
         sigma = np.zeros(K)
         _raise_for_status(_lib().hprqp_batch_get_sigma(self._handle, sigma.ctypes.data_as(c_double_p)),
                           "hprqp_batch_get_sigma")
+        seconds = np.zeros(K)
+        _raise_for_status(_lib().hprqp_batch_get_times(self._handle, seconds.ctypes.data_as(c_double_p)),
+                          "hprqp_batch_get_times")
         return BatchResult(status, it.astype(np.int64), obj, res, gap, x[:self.n], y[:self.m], z[:self.n],
-                           w[:self.n], float(_lib().hprqp_batch_last_solve_ms(self._handle)), sigma)
+                           w[:self.n], float(_lib().hprqp_batch_last_solve_ms(self._handle)), sigma, seconds)
 
     def backward(self, grad_x, grad_y=None, tol: float = 1e-12) -> Gradients:
         """Implicit-differentiation adjoint of the last solve (one MINRES

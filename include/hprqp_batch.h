@@ -71,6 +71,12 @@ HPRQPStatus hprqp_batch_set_warm_start(HPRQPBatch *batch, const double *x0, cons
 /* sigma of each instance at the end of the last hprqp_batch_solve. */
 HPRQPStatus hprqp_batch_get_sigma(const HPRQPBatch *batch, double *sigma);
 
+/* Seconds each instance of the last hprqp_batch_solve took on its CTA, from
+ * loading its data to writing its results (device clock; instances run
+ * concurrently, so these do not add up to the launch time).  The per-solve
+ * time a dataset table reports for a batched run. */
+HPRQPStatus hprqp_batch_get_times(const HPRQPBatch *batch, double *seconds);
+
 /* Device time of the last hprqp_batch_solve kernel, milliseconds. */
 double hprqp_batch_last_solve_ms(const HPRQPBatch *batch);
 size_t hprqp_batch_num_instances(const HPRQPBatch *batch);
