@@ -712,15 +712,21 @@ def model_arrays(model: Model):
 def __getattr__(name):
     """``hprqp.QPFunction`` / ``hprqp.QPLayer`` (batched) and
     ``hprqp.SingleQPFunction`` (one large QP): the differentiable layers,
-    imported on first use so that torch stays optional."""
+    imported on first use so that torch stays optional; the CVXPY bridge
+    (``build_from_cvxpy_problem``, ``solve_cvxpy_problem``), likewise."""
     if name in ("QPFunction", "QPLayer", "SingleQPFunction"):
         from . import torch_layer
 
         return getattr(torch_layer, name)
+    if name in ("CVXPYBuildInfo", "build_from_cvxpy_problem", "solve_cvxpy_problem"):
+        from . import cvxpy_bridge
+
+        return getattr(cvxpy_bridge, name)
     raise AttributeError(f"module 'hprqp' has no attribute {name!r}")
 
 
 __all__ = [
+    "CVXPYBuildInfo", "build_from_cvxpy_problem", "solve_cvxpy_problem",
     "QPFunction", "QPLayer", "SingleQPFunction", "SolveState", "residuals", "solve_for_backward", "Model", "Parameters", "Result", "SPMV_MODE_AUTO", "SPMV_MODE_CUSPARSE", "SPMV_MODE_CUSTOMIZED",
     "STATUS_ALLOCATION_FAILED", "STATUS_CONTINUE", "STATUS_INVALID_ARGUMENT", "STATUS_MAX_ITER",
     "STATUS_NOT_IMPLEMENTED", "STATUS_OK", "STATUS_OPTIMAL", "STATUS_TIME_LIMIT", "build_from_mps",
