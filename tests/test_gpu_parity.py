@@ -91,6 +91,56 @@ def test_gather_bound_checksum(engine_lib):
     assert abs(total - float(np.sum(y))) <= 1e-12 * float(np.sum(np.abs(data * x[indices])))
 
 
+def test_spmv_reference_exact_values(engine_lib):
+    """tests/gpu/test_gpu_spmv_operation.cu:27-29, 47-52: exact products of
+    a 3x3 CSR with two vectors."""
+    indptr, indices = np.array([0, 2, 3, 5]), np.array([0, 2, 1, 0, 2])
+    data = np.array([2.0, -1.0, 3.0, 4.0, 5.0])
+    y, _ = engine_lib.spmv(indptr, indices, data, 3, np.array([1.0, 2.0, 3.0]))
+    assert y.tolist() == [-1.0, 6.0, 19.0]
+    y, _ = engine_lib.spmv(indptr, indices, data, 3, np.array([-2.0, 1.0, 4.0]))
+    assert y.tolist() == [-8.0, 3.0, 12.0]
+
+
+def _packed_fixture(fixture):
+    """the eight row patterns of tests/gpu/test_gpu_packed_spmv.cu:18-22"""
+    m = {0: 1, 1: 127, 2: 257}.get(fixture, 128)
+    n = 311 if fixture == 2 else 256
+    indptr, indices, data = [0], [], []
+    for i in range(m):
+        k = {0: 2, 1: 3, 2: 7, 3: 31, 4: 33, 6: 0}.get(fixture)
+        if fixture == 5:
+            k = 32 if i == 0 else 1
+        if fixture == 7:
+            k = 0 if i % 5 == 0 else 5
+        for j in sorted({(i * 11 + t * 7) % n for t in range(k)}):
+            indices.append(j)
+            data.append(np.sin(1.7 * i + 0.3 * j))
+        indptr.append(len(indices))
+    return np.array(indptr), np.array(indices, dtype=np.int64), np.array(data), n
+
+
+@pytest.mark.parametrize("fixture", range(8))
+def test_spmv_reference_patterns(engine_lib, fixture):
+    """tests/gpu/test_gpu_packed_spmv.cu:9-14: each pattern and its
+    transpose within 1e-12 of an extended-precision sum, x_j = sin(.19 j) +
+    cos(.011 j)."""
+    import math
+
+    import scipy.sparse as sp
+
+    indptr, indices, data, n = _packed_fixture(fixture)
+    M = sp.csr_matrix((data, indices, indptr), shape=(len(indptr) - 1, n))
+    for mat in (M, M.T.tocsr()):
+        mat.sort_indices()
+        x = np.array([math.sin(0.19 * j) + math.cos(0.011 * j) for j in range(mat.shape[1])])
+        y, _ = engine_lib.spmv(mat.indptr, mat.indices, mat.data, mat.shape[1], x)
+        for i in range(mat.shape[0]):
+            s, e = mat.indptr[i], mat.indptr[i + 1]
+            ref = math.fsum(mat.data[s:e] * x[mat.indices[s:e]]) if e > s else 0.0
+            assert abs(y[i] - ref) / (1.0 + abs(ref)) < 1e-12
+
+
 def test_spmv_empty_matrix(engine_lib):
     indptr = np.zeros(11, np.int64)
     y, _ = engine_lib.spmv(indptr, np.zeros(0, np.int64), np.zeros(0), 5, np.ones(5))
