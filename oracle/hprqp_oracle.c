@@ -1190,6 +1190,21 @@ void oracle_params_default(OracleParams *p)
 int oracle_solve(const OracleModel *mo, const OracleParams *pr, OracleResult *out, double *x,
                  double *y, double *z, double *wv)
 {
+    return oracle_solve_from(mo, pr, NULL, NULL, NULL, 0.0, out, x, y, z, wv);
+}
+
+/* Warm start: this project's addition (the reference always starts at
+ * zero, its vectors zero-filled at allocation, src/gpu/context.cu:75-96),
+ * restated from the batch solver's rules so that its iterates can be
+ * checked: the iterates and the Halpern anchors start at the point scaled
+ * like the data (x0 * col_norm / b_scale, w0 likewise, y0 * row_norm /
+ * c_scale, the inverse of the output map), A'y (and Q w on the noC path)
+ * are computed once, sigma0 > 0 replaces the data-based sigma0 (clamped to
+ * [1e-12, 1e12]), and the point is not accepted as optimal at iteration 0. */
+int oracle_solve_from(const OracleModel *mo, const OracleParams *pr, const double *x0, const double *y0,
+                      const double *w0, double sigma0, OracleResult *out, double *x, double *y, double *z,
+                      double *wv)
+{
     if (!mo || !pr || !out) return ORACLE_INVALID;
     memset(out, 0, sizeof(*out));
     double t0 = o_now();
@@ -1202,6 +1217,29 @@ int oracle_solve(const OracleModel *mo, const OracleParams *pr, OracleResult *ou
         ws_free(&w);
         prob_free(&p);
         return st;
+    }
+    const int warm = x0 != NULL;
+    if (warm) {
+        if (sigma0 > 0.0) {
+            w.sigma = o_clamp(sigma0, 1e-12, 1e12);
+            if (w.Q_is_diag) update_diag_factors(&w);
+        }
+        for (size_t i = 0; i < w.n; ++i) {
+            const double cn = p.col_norm[i];
+            const double xs = x0[i] * cn / p.b_scale, ws = (w0 ? w0[i] : x0[i]) * cn / p.b_scale;
+            w.x[i] = w.x_bar[i] = w.x_hat[i] = w.last_x[i] = xs;
+            w.w[i] = w.w_bar[i] = w.last_w[i] = ws;
+        }
+        for (size_t i = 0; i < w.m; ++i)
+            w.y[i] = w.y_bar[i] = w.last_y[i] = y0 ? y0[i] * p.row_norm[i] / p.c_scale : 0.0;
+        if (w.m > 0) {
+            o_spmv(&p.AT, w.y, w.ATy);
+            for (size_t i = 0; i < w.n; ++i) w.ATy_bar[i] = w.last_ATy[i] = w.ATy[i];
+        }
+        if (w.noC) {
+            o_spmv(&p.Q, w.w, w.Qw);
+            for (size_t i = 0; i < w.n; ++i) w.Qw_bar[i] = w.last_Qw[i] = w.Qw[i];
+        }
     }
     ORes res;
     ORst rs;
@@ -1226,7 +1264,7 @@ int oracle_solve(const OracleModel *mo, const OracleParams *pr, OracleResult *ou
                 res.is_updated = 0;
             }
         }
-        if (res.kkt < pr->stoptol) final_status = ORACLE_OPTIMAL;
+        if (res.kkt < pr->stoptol && !(warm && iter == 0)) final_status = ORACLE_OPTIMAL;
         else if (iter == pr->max_iter) final_status = ORACLE_MAX_ITER;
         else if (el > pr->time_limit) final_status = ORACLE_TIME_LIMIT;
         else final_status = ORACLE_CONTINUE;

@@ -92,6 +92,14 @@ void oracle_model_export(const OracleModel *model, size_t *q_row_ptr, size_t *q_
 int oracle_solve(const OracleModel *model, const OracleParams *params, OracleResult *result,
                  double *x, double *y, double *z, double *w);
 
+/* The same solve from a warm start (x0, w0: n; y0: m rows of the
+ * preprocessed model; w0 and y0 may be NULL: x0 and zero; x0 == NULL is a
+ * cold start) and an optional sigma0 (> 0), following the batch solver's
+ * warm-start rules (an addition of this project, not in the reference). */
+int oracle_solve_from(const OracleModel *model, const OracleParams *params, const double *x0,
+                      const double *y0, const double *w0, double sigma0, OracleResult *result, double *x,
+                      double *y, double *z, double *w);
+
 /* Scaling only: fills row_norm (m), col_norm (n) and the scaled Q/A values
  * (arrays sized like the preprocessed model), plus scalars
  * [norm_b_org, norm_c_org, norm_b, norm_c]. */

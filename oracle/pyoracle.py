@@ -83,6 +83,7 @@ def lib() -> ctypes.CDLL:
         _lib = ctypes.CDLL(str(ORACLE_LIB))
         _lib.oracle_build.restype = ctypes.c_int
         _lib.oracle_solve.restype = ctypes.c_int
+        _lib.oracle_solve_from.restype = ctypes.c_int
         _lib.oracle_model_n.restype = ctypes.c_size_t
         _lib.oracle_model_m.restype = ctypes.c_size_t
         _lib.oracle_model_q_nnz.restype = ctypes.c_size_t
@@ -162,15 +163,30 @@ class OracleModel:
                     c=c, l=l, u=u, AL=AL[:self.m], AU=AU[:self.m])
 
     def solve(self, stoptol=1e-8, max_iter=2147483647, time_limit=3600.0, check_iter=100,
-              print_frequency=-1, use_scaling=True, mode=MODE_GPU_REF):
+              print_frequency=-1, use_scaling=True, mode=MODE_GPU_REF, x0=None, y0=None, w0=None, sigma0=0.0):
+        """Solve; with x0 (n), optionally y0 (m rows of the preprocessed
+        model), w0 (n) and sigma0 > 0, from that warm start
+        (oracle_solve_from)."""
         p = _OracleParams(stoptol, max_iter, time_limit, check_iter, print_frequency, int(use_scaling), mode)
         r = _OracleResult()
         x = np.zeros(max(self.n, 1))
         w = np.zeros(max(self.n, 1))
         z = np.zeros(max(self.n, 1))
         y = np.zeros(max(self.m, 1))
-        lib().oracle_solve(self.handle, ctypes.byref(p), ctypes.byref(r), x.ctypes.data_as(c_double_p),
-                           y.ctypes.data_as(c_double_p), z.ctypes.data_as(c_double_p), w.ctypes.data_as(c_double_p))
+
+        def start(a, size):
+            if a is None:
+                return None, None
+            a = np.ascontiguousarray(a, np.float64).reshape(-1)
+            if a.shape[0] != size:
+                raise ValueError(f"warm start: expected {size} entries, got {a.shape[0]}")
+            a = a if size else np.zeros(1)
+            return a, a.ctypes.data_as(c_double_p)
+
+        (xa, xp), (ya, yp), (wa, wp) = start(x0, self.n), start(y0, self.m), start(w0, self.n)
+        lib().oracle_solve_from(self.handle, ctypes.byref(p), xp, yp, wp, ctypes.c_double(sigma0), ctypes.byref(r),
+                                x.ctypes.data_as(c_double_p), y.ctypes.data_as(c_double_p),
+                                z.ctypes.data_as(c_double_p), w.ctypes.data_as(c_double_p))
         out = {name: getattr(r, name) for name, _ in _OracleResult._fields_}
         out.update(x=x[:self.n], y=y[:self.m], z=z[:self.n], w=w[:self.n])
         return out

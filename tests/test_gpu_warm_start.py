@@ -176,3 +176,34 @@ def test_qp_layer_warm_start(engine_lib):
     (xw, gw), (xc, gc) = outs
     assert np.max(np.abs(xw - xc)) <= 1e-5 * max(1.0, np.max(np.abs(xc)))
     assert np.max(np.abs(gw - gc)) <= 1e-4 * max(1.0, np.max(np.abs(gc)))
+
+
+@pytest.mark.parametrize("cap", [1, 10, 100])
+@pytest.mark.parametrize("with_sigma", [False, True])
+def test_warm_iterates_after_k_steps_match_oracle(engine_lib, cap, with_sigma):
+    """The batch's warm start against the oracle's restatement of the same
+    rules (oracle_solve_from): status, iteration count and iterates after K
+    steps within 1e-8, from a seeded random point (and sigma0 = 2)."""
+    from hprqp import batch
+
+    insts = _mixed_batch()
+    rng = np.random.default_rng(17)
+    n_tot, m_tot = sum(i.n for i in insts), sum(i.m for i in insts)
+    x0, y0, w0 = rng.standard_normal(n_tot), rng.standard_normal(m_tot), rng.standard_normal(n_tot)
+    sig = np.full(len(insts), 2.0) if with_sigma else None
+    b = batch.Batch(insts)
+    b.set_warm_start(x0, y0, w0, sig)
+    b.solve(stoptol=1e-8, max_iter=cap)
+    r = b.results()
+    b.close()
+    vo, ro = np.cumsum([0] + [i.n for i in insts]), np.cumsum([0] + [i.m for i in insts])
+    for k, inst in enumerate(insts):
+        xs, ws = slice(vo[k], vo[k + 1]), slice(vo[k], vo[k + 1])
+        kept = _kept(inst)
+        yk = y0[ro[k]:ro[k + 1]][kept]
+        o = pyoracle.OracleModel(inst).solve(stoptol=1e-8, max_iter=cap, mode=pyoracle.MODE_GPU_REF,
+                                             x0=x0[xs], y0=yk, w0=w0[ws], sigma0=2.0 if with_sigma else 0.0)
+        assert r.status[k] == o["status"] and r.iter[k] == o["iter"], (k, r.status[k], o["status"], r.iter[k])
+        got_y = r.y[ro[k]:ro[k + 1]][kept]
+        for got, ref in ((r.x[xs], o["x"]), (got_y, o["y"]), (r.z[xs], o["z"]), (r.w[ws], o["w"])):
+            assert np.max(np.abs(got - ref)) <= 1e-8 * max(1.0, float(np.max(np.abs(ref)))), k
