@@ -90,3 +90,19 @@ def test_batch_flag_selects_the_batched_solver(tmp_path, monkeypatch):
 
 def test_missing_folder(tmp_path):
     assert dataset.run(tmp_path / "nope", tmp_path / "out", _args()) == 1
+
+
+def test_failed_status_and_missing_clocks(tmp_path):
+    """the reference's tests/test_dataset.py:110-120: an unsolved file counts
+    as the time limit, a solved file without a process clock empties that
+    mean, and the solved count is 1"""
+    out = tmp_path / "a.csv"
+    dataset.write_table(out, [{"name": "success", "status": "OPTIMAL", "alg_time": "1200"},
+                              {"name": "fail", "status": "TIME_LIMIT", "alg_time": "2"}], 1000)
+    import csv
+
+    with out.open() as f:
+        rows = list(csv.DictReader(f))
+    assert float(rows[-2]["alg_time"]) == pytest.approx((1210 * 1010) ** 0.5 - 10, abs=1e-7)
+    assert rows[-2]["process_time"] == ""
+    assert rows[-1]["alg_time"] == "1"
