@@ -8,6 +8,8 @@
 // per-row merge of Q's row and Q''s row instead of a global sort of all
 // entries, and the bounds/column-range checks run before anything is copied.
 #include "hprqp.h"
+#include "shared/build.h"
+#include "shared/vector.h"
 
 #include <algorithm>
 #include <cmath>
@@ -358,6 +360,8 @@ static HPRQPStatus validate_cones(const HPRQPModel *model)
     if (!cone_offsets_ok(model->num_var_cones, model->var_cone_offsets, n) ||
         !cone_offsets_ok(model->num_row_cones, model->row_cone_offsets, m))
         return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (model->num_var_cones && (!model->l || !model->u)) return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (model->num_row_cones && (!model->AL || !model->AU)) return HPRQP_STATUS_INVALID_ARGUMENT;
     if (model->num_var_cones)
         for (size_t i = model->var_cone_offsets[0]; i < n; ++i)
             if (model->l[i] != -INFINITY || model->u[i] != INFINITY) return HPRQP_STATUS_INVALID_ARGUMENT;
@@ -414,6 +418,79 @@ HPRQPStatus build_from_QAbc_soc(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A
     st = validate_cones(model);
     if (st != HPRQP_STATUS_OK) model_free(model);
     return st;
+}
+
+// The reference's lower-level builder entry points (include/shared/build.h,
+// src/shared/build.c:39-99, 339-400, 594-600): build_model_from_arrays is
+// build_from_QAbc; preprocess_model redoes the builder's checks and
+// reductions on a model that already owns its arrays.
+HPRQPStatus build_model_from_arrays(const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c,
+                                    const double *AL, const double *AU, const double *l, const double *u,
+                                    double obj_constant, HPRQPModel *model)
+{
+    return build_impl(Q, A, c, AL, AU, l, u, obj_constant, false, model);
+}
+
+HPRQPStatus model_validate_soc(const HPRQPModel *model)
+{
+    return model ? validate_cones(model) : HPRQP_STATUS_INVALID_ARGUMENT;
+}
+
+HPRQPStatus preprocess_model(HPRQPModel *model)
+{
+    if (!model || !model->owns_data || !matrix_csr_is_valid(&model->AT)) return HPRQP_STATUS_INVALID_ARGUMENT;
+    HPRQPStatus st = validate_cones(model);
+    if (st != HPRQP_STATUS_OK) return st;
+    const bool cones = model->num_var_cones || model->num_row_cones;
+    // rebuild from the model's own arrays (cone models keep every row), then
+    // hand the cone blocks over unchanged
+    HPRQPModel out;
+    model_init(&out);
+    st = build_impl(&model->Q, &model->A, model->c, model->AL, model->AU, model->l, model->u, model->obj_constant,
+                    cones, &out);
+    if (st != HPRQP_STATUS_OK) return st;
+    out.num_var_cones = model->num_var_cones;
+    out.var_cone_offsets = model->var_cone_offsets;
+    out.num_row_cones = model->num_row_cones;
+    out.row_cone_offsets = model->row_cone_offsets;
+    out.soc_rhs = model->soc_rhs;
+    model->var_cone_offsets = model->row_cone_offsets = nullptr;
+    model->soc_rhs = nullptr;
+    model_free(model);
+    *model = out;
+    return HPRQP_STATUS_OK;
+}
+
+// vector helpers (include/shared/vector.h; reference src/shared/vector.c)
+void vec_fill(double *x, size_t n, double value) { std::fill(x, x + n, value); }
+
+void vec_copy(double *dest, const double *src, size_t n) { std::copy(src, src + n, dest); }
+
+void vec_axpby(double *y, const double *x, size_t n, double a, double b)
+{
+    for (size_t i = 0; i < n; ++i) y[i] = a * x[i] + b * y[i];
+}
+
+double vec_dot(const double *x, const double *y, size_t n)
+{
+    double s = 0.0;
+    for (size_t i = 0; i < n; ++i) s += x[i] * y[i];
+    return s;
+}
+
+double vec_norm2(const double *x, size_t n) { return std::sqrt(vec_dot(x, x, n)); }
+
+double vec_norm_inf(const double *x, size_t n)
+{
+    double m = 0.0;
+    for (size_t i = 0; i < n; ++i)
+        if (std::fabs(x[i]) > m) m = std::fabs(x[i]);
+    return m;
+}
+
+void vec_project_box(double *y, const double *x, const double *lower, const double *upper, size_t n)
+{
+    for (size_t i = 0; i < n; ++i) y[i] = std::min(std::max(x[i], lower[i]), upper[i]);
 }
 
 // build_from_mps lives in mps.cpp

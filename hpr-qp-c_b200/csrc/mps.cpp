@@ -489,3 +489,10 @@ extern "C" HPRQPStatus build_from_mps(const char *mps_path, HPRQPModel *model)
                            m ? R.up_row.data() : nullptr, l.empty() ? &one : l.data(), u.empty() ? &one : u.data(),
                            R.c0, model);
 }
+
+// the reference's name for the same reader (include/shared/build.h;
+// src/shared/mps_qp.cpp:208, which its build_from_mps calls)
+extern "C" HPRQPStatus build_model_from_mps(const char *mps_path, HPRQPModel *model)
+{
+    return build_from_mps(mps_path, model);
+}
