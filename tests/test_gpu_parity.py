@@ -273,3 +273,26 @@ def test_residual_kernels_match_oracle(engine_lib, scaling):
     k = pyoracle.OracleModel(inst).kkt(x, y, z)
     for key in ("err_rp", "err_rd", "gap", "primal_obj", "dual_obj"):
         assert abs(r[key] - k[key]) <= 1e-10 * max(1.0, abs(k[key])), (key, r[key], k[key])
+
+
+def test_reference_mps_fixture_through_binding(engine_lib):
+    """tests/test_binding_api.c:16-118 of the reference on its own
+    simple_qp.mps: 2 variables and 2 rows, max_iter 0 gives MAX_ITER with
+    solution vectors; solved to 1e-8 it matches the reference CPU solver's
+    result recorded in tests/golden/simple_qp.json."""
+    import json
+    from pathlib import Path
+
+    hprqp = engine_lib
+    golden = Path(__file__).resolve().parent / "golden"
+    ref = json.loads((golden / "simple_qp.json").read_text())
+    model = hprqp.read_from_mps(golden / "simple_qp.mps")
+    assert (model.num_variables, model.num_constraints) == (2, 2)
+    r0 = hprqp.optimize(model, hprqp.Parameters(verbose=False, max_iter=0))
+    assert r0.status_code == hprqp.STATUS_MAX_ITER == ref["max_iter0"]["status"]
+    assert len(r0.x) == 2 and len(r0.y) == 2
+    r = hprqp.optimize(model, hprqp.Parameters(verbose=False, stoptol=1e-8))
+    want = ref["solve_1e-8"]
+    assert r.status_code == want["status"] == hprqp.STATUS_OPTIMAL
+    assert abs(r.objective - want["primal_obj"]) <= 1e-6 * max(1.0, abs(want["primal_obj"]))
+    assert np.allclose(r.x, want["x"], atol=1e-5) and np.allclose(r.y, want["y"], atol=1e-5)

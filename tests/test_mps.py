@@ -4,6 +4,8 @@ libraries must return bit-identical models, and reject the same malformed
 files."""
 from __future__ import annotations
 
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -83,3 +85,19 @@ def test_solve_from_mps_matches_arrays(engine_lib, tmp_path):
     r2 = hprqp.optimize(m2, hprqp.Parameters(verbose=False, stoptol=1e-6))
     assert r1.status_code == r2.status_code == hprqp.STATUS_OPTIMAL
     assert abs(r1.objective - r2.objective) <= 1e-6 * abs(r2.objective)
+
+
+def test_reference_fixture_model(engine_lib):
+    """the reference's own tests/data/simple_qp.mps: the model equals what
+    the reference's reader built from it (tests/golden/simple_qp.json, made
+    by tests/golden/make_reference_fixtures.py)"""
+    import json
+
+    golden = Path(__file__).resolve().parent / "golden"
+    ref = json.loads((golden / "simple_qp.json").read_text())["model"]
+    got = engine_lib.read_from_mps(golden / "simple_qp.mps").to_instance()
+    assert (got.n, got.m) == (ref["n"], ref["m"]) and got.obj_constant == ref["obj_constant"]
+    for mine, key in ((got.Q.indptr, "q_indptr"), (got.Q.indices, "q_indices"), (got.Q.data, "q_data"),
+                      (got.A.indptr, "a_indptr"), (got.A.indices, "a_indices"), (got.A.data, "a_data"),
+                      (got.c, "c"), (got.l, "l"), (got.u, "u"), (got.AL, "AL"), (got.AU, "AU")):
+        assert np.array_equal(np.asarray(mine, float), np.asarray(ref[key], float)), key
