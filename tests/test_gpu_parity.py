@@ -194,6 +194,20 @@ def test_iterates_after_k_steps(engine_lib, inst, cap):
         assert _rel(getattr(r, key), o[key]) <= 1e-8, key
 
 
+@pytest.mark.parametrize("inst", TINY, ids=[i.name for i in TINY])
+@pytest.mark.parametrize("cap", [1, 10])
+def test_steps_within_reference_iteration_tolerance(engine_lib, inst, cap):
+    """the reference's GPU-vs-CPU step tolerance, 1e-12 absolute
+    (tests/gpu/test_gpu_iteration.cpp:42-90), on the whole solve after 1
+    and 10 steps (setup, scaling and power iterations included); measured
+    differences are at most a few 1e-16"""
+    r, o = _solve_pair(engine_lib, inst, stoptol=1e-8, max_iter=cap)
+    assert r.status_code == o["status"] and r.iter == o["iter"]
+    for key in ("x", "y", "z", "w"):
+        got, ref = np.asarray(getattr(r, key), float), np.asarray(o[key], float)
+        assert got.shape == ref.shape and (got.size == 0 or np.max(np.abs(got - ref)) <= 1e-12), key
+
+
 @pytest.mark.parametrize("inst", [i for i in TINY if i.name != "tall_diag"],
                          ids=[i.name for i in TINY if i.name != "tall_diag"])
 def test_tiny_solves_converge_like_oracle(engine_lib, inst):
