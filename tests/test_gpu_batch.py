@@ -52,6 +52,26 @@ def test_batch_iterates_after_k_steps(engine_lib, cap):
             assert _rel(got, ref) <= 1e-8, inst.name
 
 
+@pytest.mark.parametrize("cap", [1, 10])
+def test_batch_steps_within_reference_iteration_tolerance(engine_lib, cap):
+    """the reference's GPU-vs-CPU step tolerance, 1e-12 absolute
+    (tests/gpu/test_gpu_iteration.cpp:42-90), for every fixture model solved
+    in one batch; measured differences are at most a few 1e-15"""
+    from hprqp import batch
+
+    insts = instances.tiny_cases()
+    b = batch.Batch(insts)
+    b.solve(stoptol=1e-8, max_iter=cap)
+    r = b.results()
+    b.close()
+    xs, ys, zs, ws = b.split(r.x, "x"), b.split(r.y, "y"), b.split(r.z, "x"), b.split(r.w, "x")
+    for k, inst in enumerate(insts):
+        o = pyoracle.OracleModel(inst).solve(stoptol=1e-8, max_iter=cap, mode=pyoracle.MODE_GPU_REF)
+        assert r.status[k] == o["status"] and r.iter[k] == o["iter"], inst.name
+        for got, ref in ((xs[k], o["x"]), (ys[k][_kept(inst)], o["y"]), (zs[k], o["z"]), (ws[k], o["w"])):
+            assert len(ref) == 0 or np.max(np.abs(got - ref)) <= 1e-12, inst.name
+
+
 def test_batch_tiny_converge(engine_lib):
     from hprqp import batch
 
