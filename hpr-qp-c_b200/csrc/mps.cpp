@@ -17,15 +17,19 @@
 //     gets upper bound inf;
 //   * numbers may use a Fortran 'D' exponent; names are free-format tokens;
 //   * duplicate (row, column) entries are summed.
+//   * QCMATRIX <row> blocks (after COLUMNS, one per constraint row) give
+//     x'Hx for that row; like the reference's file loader only diagonal H
+//     is accepted, on one-sided rows, convex in the row's sense; such rows
+//     become second-order cones through build_from_QAbc_qc_diagonal
+//     (qcqp.cpp), the other rows keep their order.
 // Discrete variables (integer markers, BV/LI/UI bounds) and maximisation are
-// rejected with HPRQP_STATUS_INVALID_ARGUMENT like the reference; quadratic
-// constraints (QCMATRIX) return HPRQP_STATUS_NOT_IMPLEMENTED: this engine
-// has no quadratic-constraint path.
+// rejected with HPRQP_STATUS_INVALID_ARGUMENT like the reference.
 //
 // The implementation is this project's: a line tokenizer over std::string
 // views, hash maps for names, COO triplets sorted stably into CSR, then the
 // same builder as build_from_QAbc (model.cpp).
 #include "hprqp.h"
+#include "shared/qcqp.h"
 
 #include <algorithm>
 #include <cerrno>
@@ -60,6 +64,8 @@ struct Reader {
     std::vector<double> c, lo_var, up_var;
     std::vector<char> discrete;
     std::vector<Triplet> a, q;
+    std::vector<std::vector<std::pair<size_t, double>>> qc;  // per constraint row: (column, x'Hx coefficient)
+    int qc_row = -1;                                          // row of the current QCMATRIX block
     double c0 = 0.0;
     bool have_obj = false, maximize = false, full_q = false, quadratic_rows = false;
     std::string rhs_set, rng_set, bnd_set;
@@ -280,9 +286,17 @@ bool data_line(Reader &R, Sec sec, const std::vector<std::string> &t, bool &inte
         R.q.push_back({i1->second, i2->second, v1});
         return true;
     }
-    case Sec::Qcmatrix:
-        R.quadratic_rows = true;
+    case Sec::Qcmatrix: {
+        // reference src/shared/mps_reader.cpp:968-990
+        if (nf != 3 || !parse_number(t[2], &v1)) return R.fail("invalid QCMATRIX coefficient");
+        auto i1 = R.cols.find(t[0]), i2 = R.cols.find(t[1]);
+        if (i1 == R.cols.end() || i2 == R.cols.end()) return R.fail("unknown column in QCMATRIX");
+        if (i1->second != i2->second && v1 != 0.0)
+            return R.fail("non-diagonal QCMATRIX entries are not supported by the MPS reader; use "
+                          "build_from_QAbc_qc_factors with a factor of the matrix");
+        if (v1 != 0.0) R.qc[(size_t)R.qc_row].push_back({(size_t)i1->second, v1});
         return true;
+    }
     default:
         return R.fail("data outside a section");
     }
@@ -398,6 +412,8 @@ bool read_file(const char *path, Reader &R)
                     if (qc_rows[it->second - 1]) ok = R.fail("second QCMATRIX block for a row");
                     qc_rows[it->second - 1] = 1;
                     R.quadratic_rows = true;
+                    if (R.qc.empty()) R.qc.resize(R.kind.size());
+                    R.qc_row = it->second - 1;
                 }
                 sec = Sec::Qcmatrix;
             } else if (h == "ENDATA") {
@@ -417,6 +433,91 @@ bool read_file(const char *path, Reader &R)
     fclose(fp);
     if (ok && !ended) ok = R.fail("end of file before ENDATA");
     return ok;
+}
+
+// Quadratic rows (reference src/shared/mps_qp.cpp:119-206).  Each row's
+// entries are sorted by (column, value), equal columns summed in that order,
+// zeros dropped; a row left empty stays linear.  Otherwise the row must be
+// one-sided: AL = -inf (sign +1) or AU = +inf (sign -1); D = 2 sign H must
+// be >= 0 and finite; C = sign a_r; constant = -AU (sign +1) or AL (sign
+// -1).  Returns false when no row is quadratic (the caller builds a QP).
+bool build_quadratic_rows(const Reader &R, const HPRQPMatrixCSR *Q, const std::vector<size_t> &arp,
+                          const std::vector<size_t> &aci, const std::vector<double> &av, const double *c,
+                          const double *l, const double *u, HPRQPModel *model, HPRQPStatus *status)
+{
+    const size_t m = R.kind.size(), n = R.c.size();
+    std::vector<std::vector<std::pair<size_t, double>>> diag(m);
+    std::vector<double> sign(m, 1.0);
+    size_t nq = 0;
+    for (size_t r = 0; r < m && r < R.qc.size(); ++r) {
+        auto d = R.qc[r];
+        std::sort(d.begin(), d.end());
+        size_t w = 0;
+        for (const auto &e : d) {
+            if (w && d[w - 1].first == e.first) d[w - 1].second += e.second;
+            else d[w++] = e;
+        }
+        d.resize(w);
+        d.erase(std::remove_if(d.begin(), d.end(), [](const std::pair<size_t, double> &e) { return e.second == 0.0; }),
+                d.end());
+        if (d.empty()) continue;
+        const double lo = R.lo_row[r], up = R.up_row[r];
+        if (lo == -INFINITY && std::isfinite(up)) sign[r] = 1.0;
+        else if (up == INFINITY && std::isfinite(lo)) sign[r] = -1.0;
+        else {
+            fprintf(stderr, "hprqp-b200: a QCMATRIX row needs a one-sided inequality (not an equality, range or "
+                            "free row)\n");
+            *status = HPRQP_STATUS_INVALID_ARGUMENT;
+            return true;
+        }
+        for (auto &e : d) {
+            e.second *= 2.0 * sign[r];
+            if (!std::isfinite(e.second) || e.second < 0.0) {
+                fprintf(stderr, "hprqp-b200: a QCMATRIX row is not convex in its inequality sense\n");
+                *status = HPRQP_STATUS_INVALID_ARGUMENT;
+                return true;
+            }
+        }
+        diag[r] = std::move(d);
+        ++nq;
+    }
+    if (nq == 0) return false;
+    std::vector<size_t> lrp(1, 0), lci, crp(1, 0), cci, drp(1, 0), dci;
+    std::vector<double> lv, cv, dv, constant, al, au;
+    for (size_t r = 0; r < m; ++r) {
+        if (diag[r].empty()) {
+            for (size_t k = arp[r]; k < arp[r + 1]; ++k) {
+                lci.push_back(aci[k]);
+                lv.push_back(av[k]);
+            }
+            lrp.push_back(lci.size());
+            al.push_back(R.lo_row[r]);
+            au.push_back(R.up_row[r]);
+        } else {
+            for (size_t k = arp[r]; k < arp[r + 1]; ++k) {
+                cci.push_back(aci[k]);
+                cv.push_back(sign[r] * av[k]);
+            }
+            crp.push_back(cci.size());
+            for (const auto &e : diag[r]) {
+                dci.push_back(e.first);
+                dv.push_back(e.second);
+            }
+            drp.push_back(dci.size());
+            constant.push_back(sign[r] > 0.0 ? -R.up_row[r] : R.lo_row[r]);
+        }
+    }
+    size_t zi = 0;
+    double zv = 0.0;
+    auto pi = [&zi](std::vector<size_t> &x) { return x.empty() ? &zi : x.data(); };
+    auto pv = [&zv](std::vector<double> &x) { return x.empty() ? &zv : x.data(); };
+    HPRQPMatrixCSR lin{lrp.size() - 1, n, lci.size(), lrp.data(), pi(lci), pv(lv), 0};
+    HPRQPMatrixCSR C{nq, n, cci.size(), crp.data(), pi(cci), pv(cv), 0};
+    HPRQPMatrixCSR D{nq, n, dci.size(), drp.data(), pi(dci), pv(dv), 0};
+    *status = build_from_QAbc_qc_diagonal(Q, &lin, c, al.empty() ? nullptr : al.data(),
+                                          au.empty() ? nullptr : au.data(), l, u, R.c0, &C, constant.data(), &D,
+                                          model);
+    return true;
 }
 
 }  // namespace
@@ -449,10 +550,6 @@ extern "C" HPRQPStatus build_from_mps(const char *mps_path, HPRQPModel *model)
             fprintf(stderr, "hprqp-b200: discrete MPS variables are not supported\n");
             return HPRQP_STATUS_INVALID_ARGUMENT;
         }
-    if (R.quadratic_rows) {
-        fprintf(stderr, "hprqp-b200: QCMATRIX (quadratic constraints) is not supported by this engine\n");
-        return HPRQP_STATUS_NOT_IMPLEMENTED;
-    }
     std::vector<size_t> arp, aci, qrp, qci;
     std::vector<double> av, qv;
     to_csr(m, n, R.a, arp, aci, av);
@@ -485,6 +582,12 @@ extern "C" HPRQPStatus build_from_mps(const char *mps_path, HPRQPModel *model)
     HPRQPMatrixCSR A{m, n, av.size(), arp.data(), aci.empty() ? &dummy_i : nz(aci), av.empty() ? &dummy_s : nzd(av), 0};
     std::vector<double> cc(R.c), l(R.lo_var), u(R.up_var);
     double one = 0.0;
+    if (R.quadratic_rows) {
+        HPRQPStatus st = HPRQP_STATUS_OK;
+        if (build_quadratic_rows(R, &Q, arp, aci, av, cc.empty() ? &one : cc.data(), l.empty() ? &one : l.data(),
+                                 u.empty() ? &one : u.data(), model, &st))
+            return st;
+    }
     return build_from_QAbc(&Q, &A, cc.empty() ? &one : cc.data(), m ? R.lo_row.data() : nullptr,
                            m ? R.up_row.data() : nullptr, l.empty() ? &one : l.data(), u.empty() ? &one : u.data(),
                            R.c0, model);

@@ -704,9 +704,13 @@ def model_arrays(model: Model):
 
     q = csr(ms.Q)
     a = csr(ms.A)
+    nrc = int(ms.num_row_cones)
     return dict(n=n, m=m, q_indptr=q[0], q_indices=q[1], q_data=q[2], a_indptr=a[0], a_indices=a[1], a_data=a[2],
                 c=vec(ms.c, n), l=vec(ms.l, n), u=vec(ms.u, n), AL=vec(ms.AL, m), AU=vec(ms.AU, m),
-                obj_constant=float(ms.obj_constant))
+                obj_constant=float(ms.obj_constant), num_var_cones=int(ms.num_var_cones), num_row_cones=nrc,
+                row_cone_offsets=(np.ctypeslib.as_array(ms.row_cone_offsets, shape=(nrc + 1,)).astype(np.int64)
+                                  if nrc else np.zeros(0, np.int64)),
+                soc_rhs=vec(ms.soc_rhs, m) if nrc else np.zeros(0))
 
 
 def __getattr__(name):

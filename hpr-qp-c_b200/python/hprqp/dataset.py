@@ -17,12 +17,14 @@ persistent kernel (``hprqp_batch.h``; ``alg_time`` is then the instance's
 own time on its CTA, ``hprqp_batch_get_times``, and the ``iter_4`` /
 ``iter_6`` columns stay empty because the batch does not record them).
 
-Differences from the reference's table: a file the reader rejects (for
-example one with a QCMATRIX section, which this library does not read)
-gets the reader's status name (``NOT_IMPLEMENTED``, ``INVALID_ARGUMENT``)
-where the reference writes ``EXIT_<code>``; ``gram_active``,
-``polish_attempts`` and ``polish_accepted`` are 0 (no Gram path and no
-polishing here); ``input_format`` is ``mps`` and ``row_cones`` 0.
+Differences from the reference's table: a file the reader rejects gets the
+reader's status name (``INVALID_ARGUMENT``, ...) where the reference writes
+``EXIT_<code>``; ``gram_active``, ``polish_attempts`` and
+``polish_accepted`` are 0 (no Gram path and no polishing here).  As in the
+reference, ``input_format`` is ``mps_qcmatrix_v1`` (the reader lifts
+diagonal QCMATRIX rows to second-order cones) and ``row_cones`` counts the
+lifted cones.  With ``--batch``, files whose models have cones are solved
+one by one (the batch kernel takes QPs only).
 """
 from __future__ import annotations
 
@@ -40,7 +42,7 @@ LOG_NAME = "HPRQP_log.txt"
 SUMMARY_NAMES = ("SGM10", "solved")
 SOLVED = ("OPTIMAL", "polished_optimal")
 FINAL = SOLVED + ("OK", "MAX_ITER", "TIME_LIMIT")
-INPUT_FORMAT = "mps"
+INPUT_FORMAT = "mps_qcmatrix_v1"
 FIELDNAMES = ["name", "iter", "alg_time", "res", "primal_obj", "gap", "status", "iter_4", "time_4", "iter_6",
               "time_6", "process_time", "total_time", "gram_active", "polish_attempts", "polish_accepted",
               "input_format", "row_cones"]
@@ -111,9 +113,10 @@ def has_qcmatrix(path: Path) -> bool:
 
 
 def keep_previous(row: Dict[str, str], path: Path) -> bool:
-    """A previous row stands if its status is final and its file is one this
-    reader reads in full (no QCMATRIX section)."""
-    return row.get("status") in FINAL and not has_qcmatrix(path)
+    """A previous row stands if its status is final and it was made by a
+    reader that reads QCMATRIX sections, or its file has none (the
+    reference's can_resume, scripts/run_dataset.py:118-122)."""
+    return row.get("status") in FINAL and (row.get("input_format") == INPUT_FORMAT or not has_qcmatrix(path))
 
 
 def _row(name: str, **kw) -> Dict[str, str]:
@@ -156,8 +159,6 @@ def _read(path: Path, log: Path):
 
 def solve_each(paths: List[Path], args, log: Path) -> List[Dict[str, str]]:
     """One solve_gpu call per file (the reference's path)."""
-    from . import optimize
-
     rows = []
     for i, path in enumerate(paths, 1):
         _log(log, f"[{datetime.now():%Y-%m-%d %H:%M:%S}] solving problem {i}: {path.name}")
@@ -166,15 +167,21 @@ def solve_each(paths: List[Path], args, log: Path) -> List[Dict[str, str]]:
         if model is None:
             rows.append(_row(path.name, status=failed, process_time=time.perf_counter() - t0))
             continue
-        t1 = time.perf_counter()
-        r = optimize(model, _params(args))
-        t2 = time.perf_counter()
-        _log(log, f"iter: {r.iter}\ntime: {r.time:.12g}\nresidual: {r.residual:.12g}\nobjective: "
-                  f"{r.objective:.12g}\ngap: {r.gap:.12g}\nstatus: {r.status}")
-        rows.append(_row(path.name, iter=r.iter, alg_time=r.time, res=r.residual, primal_obj=r.objective,
-                         gap=r.gap, status=r.status, iter_4=r.iter_4, time_4=r.time_4, iter_6=r.iter_6,
-                         time_6=r.time_6, process_time=t2 - t0, total_time=t2 - t1))
+        rows.append(_solve_model(path.name, model, args, log, t0))
     return rows
+
+
+def _solve_model(name: str, model, args, log: Path, t0: float) -> Dict[str, str]:
+    from . import optimize
+
+    t1 = time.perf_counter()
+    r = optimize(model, _params(args))
+    t2 = time.perf_counter()
+    _log(log, f"iter: {r.iter}\ntime: {r.time:.12g}\nresidual: {r.residual:.12g}\nobjective: "
+              f"{r.objective:.12g}\ngap: {r.gap:.12g}\nstatus: {r.status}")
+    return _row(name, iter=r.iter, alg_time=r.time, res=r.residual, primal_obj=r.objective, gap=r.gap,
+                status=r.status, iter_4=r.iter_4, time_4=r.time_4, iter_6=r.iter_6, time_6=r.time_6,
+                process_time=t2 - t0, total_time=t2 - t1, row_cones=int(model._struct().num_row_cones))
 
 
 def solve_batched(paths: List[Path], args, log: Path) -> List[Dict[str, str]]:
@@ -189,6 +196,11 @@ def solve_batched(paths: List[Path], args, log: Path) -> List[Dict[str, str]]:
         model, failed = _read(path, log)
         if model is None:
             rows[path.name] = _row(path.name, status=failed, process_time=time.perf_counter() - t0)
+            continue
+        st = model._struct()
+        if st.num_row_cones or st.num_var_cones:
+            _log(log, f"{path.name}: cone model, solved on its own")
+            rows[path.name] = _solve_model(path.name, model, args, log, t0)
             continue
         insts.append(model.to_instance(path.name))
         t_read[path.name] = time.perf_counter() - t0

@@ -583,7 +583,10 @@ if st == 0:
     out.update(n=n, m=m, q_indptr=ii(ms.Q.row_ptr, n + 1), q_indices=ii(ms.Q.col_ind, ms.Q.nnz),
                q_data=h(ms.Q.values, ms.Q.nnz), a_indptr=ii(ms.A.row_ptr, m + 1), a_indices=ii(ms.A.col_ind, ms.A.nnz),
                a_data=h(ms.A.values, ms.A.nnz), c=h(ms.c, n), l=h(ms.l, n), u=h(ms.u, n), AL=h(ms.AL, m),
-               AU=h(ms.AU, m), obj_constant=float(ms.obj_constant).hex())
+               AU=h(ms.AU, m), obj_constant=float(ms.obj_constant).hex(),
+               num_row_cones=int(ms.num_row_cones),
+               row_cone_offsets=ii(ms.row_cone_offsets, ms.num_row_cones + 1) if ms.num_row_cones else [],
+               soc_rhs=h(ms.soc_rhs, m) if ms.num_row_cones else [], num_var_cones=int(ms.num_var_cones))
     L.model_free(ctypes.byref(ms))
 print("@@" + json.dumps(out))
 """
@@ -614,4 +617,8 @@ def ref_build_from_mps(path) -> dict:
         out[k] = np.asarray(d[k], np.int64)
     for k in ("q_data", "a_data", "c", "l", "u", "AL", "AU"):
         out[k] = np.array([float.fromhex(v) for v in d[k]], np.float64)
+    out["num_var_cones"] = int(d.get("num_var_cones", 0))
+    out["num_row_cones"] = int(d.get("num_row_cones", 0))
+    out["row_cone_offsets"] = np.asarray(d.get("row_cone_offsets", []), np.int64)
+    out["soc_rhs"] = np.array([float.fromhex(v) for v in d.get("soc_rhs", [])], np.float64)
     return out

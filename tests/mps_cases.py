@@ -165,3 +165,64 @@ def write_instance(inst) -> str:
                 out.append(f"    X{i} X{j} {float(q.data[e])!r}")
     out.append("ENDATA")
     return "\n".join(out) + "\n"
+
+
+def random_qcqp_mps(seed: int, n: int = 8, m: int = 6) -> str:
+    """A convex QCQP in free MPS: QUADOBJ diagonal objective, L and G rows
+    with diagonal QCMATRIX blocks (positive on L rows, negative on G rows,
+    a repeated entry to be summed, a zero entry to be dropped), one block of
+    zeros only (the row stays linear), an E row and a ranged row without
+    quadratic terms; x = 0 is feasible."""
+    rng = np.random.default_rng(seed)
+    cols = [f"X{j}" for j in range(n)]
+    kinds = ["L", "G", "L", "G", "E", "L"] + [rng.choice(["L", "G"]) for _ in range(m - 6)]
+    A = (rng.random((m, n)) < 0.5) * np.round(rng.standard_normal((m, n)), 3)
+    out = ["NAME QCQP%d" % seed, "ROWS", " N  OBJ"] + [f" {k}  R{i}" for i, k in enumerate(kinds)]
+    out.append("COLUMNS")
+    c = np.round(rng.standard_normal(n), 3)
+    for j, col in enumerate(cols):
+        out.append(f"    {col}  OBJ  {float(c[j])!r}")
+        for i in range(m):
+            if A[i, j] != 0:
+                out.append(f"    {col}  R{i}  {float(A[i, j])!r}")
+    out.append("RHS")
+    for i, k in enumerate(kinds):
+        v = {"L": 1.0 + rng.random(), "G": -1.0 - rng.random(), "E": 0.0}[k]
+        out.append(f"    RHS  R{i}  {float(v)!r}")
+    out += ["RANGES", "    RNG  R5  2.5"]
+    out += ["BOUNDS"] + [f" LO BND {col} -2" for col in cols[: n // 2]] + [f" FR BND {col}" for col in cols[n // 2:]]
+    out.append("QUADOBJ")
+    out += [f"    {col}  {col}  {float(1.0 + rng.random())!r}" for col in cols]
+    for i in range(4):
+        sgn = 1.0 if kinds[i] == "L" else -1.0
+        out.append(f"QCMATRIX  R{i}")
+        for j in sorted(rng.choice(n, size=3, replace=False)):
+            out.append(f"    X{j}  X{j}  {float(sgn * (0.5 + rng.random()))!r}")
+        out.append(f"    X{j}  X{j}  {sgn * 0.25!r}")  # a second entry for the same column
+        out.append(f"    X0  X1  0.0")  # an explicit zero off the diagonal: ignored
+    out += [f"QCMATRIX  R{m - 1}", "    X2  X2  0.0"]  # zeros only: the row stays linear
+    out.append("ENDATA")
+    return "\n".join(out) + "\n"
+
+
+def malformed_qcqp() -> dict:
+    """name -> QCMATRIX misuse that both readers must reject."""
+    head = ["NAME T", "ROWS", " N obj", " L c1", " G c2", " E c3", "COLUMNS", "    x obj 1 c1 1",
+            "    x c2 1 c3 1", "    y c1 1 c2 1", "RHS", "    rhs c1 4 c2 -1", "    rhs c3 0.5"]
+    end = ["ENDATA"]
+    blocks = {
+        "on_equality_row": ["QCMATRIX c3", "    x x 1"],
+        "ranged_row": ["RANGES", "    rng c1 2", "QCMATRIX c1", "    x x 1"],
+        "nonconvex_le": ["QCMATRIX c1", "    x x -1"],
+        "nonconvex_ge": ["QCMATRIX c2", "    x x 1"],
+        "off_diagonal": ["QCMATRIX c1", "    x y 1", "    y x 1"],
+        "unknown_column": ["QCMATRIX c1", "    z z 1"],
+        "objective_row": ["QCMATRIX obj", "    x x 1"],
+        "duplicate_block": ["QCMATRIX c1", "    x x 1", "QCMATRIX c1", "    y y 1"],
+        "bad_number": ["QCMATRIX c1", "    x x 1.2.3"],
+        "two_fields": ["QCMATRIX c1", "    x 1"],
+    }
+    out = {k: "\n".join(head + v + end) + "\n" for k, v in blocks.items()}
+    out["before_columns"] = "\n".join(["NAME T", "ROWS", " N obj", " L c1", "QCMATRIX c1", "    x x 1",
+                                       "COLUMNS", "    x obj 1 c1 1", "ENDATA"]) + "\n"
+    return out

@@ -61,11 +61,19 @@ def test_resume_solves_only_what_is_not_final(tmp_path, monkeypatch):
     out = tmp_path / "out"
     assert dataset.run(data, out, _args()) == 0
     assert calls == [["a.mps", "b.mps", "q.mps"]]
-    # a.mps is final; b.mps failed; q.mps has a QCMATRIX section, which this
-    # reader does not read, so its row never stands
+    # a.mps and q.mps are final; b.mps failed
     status["b.mps"] = "OPTIMAL"
     assert dataset.run(data, out, _args()) == 0
-    assert calls[1] == ["b.mps", "q.mps"]
+    assert calls[1] == ["b.mps"]
+    # a QCMATRIX file's row from a reader that did not read QCMATRIX (no
+    # input_format) does not stand, as in the reference
+    rows = dataset.read_table(out / dataset.CSV_NAME)
+    for r in rows:
+        if r["name"] == "q.mps":
+            r["input_format"] = ""
+    dataset.write_table(out / dataset.CSV_NAME, rows, 3600.0)
+    assert dataset.run(data, out, _args()) == 0
+    assert calls[2] == ["q.mps"]
     rows = dataset.read_table(out / dataset.CSV_NAME)
     assert [r["name"] for r in rows] == ["a.mps", "b.mps", "q.mps"]
     assert all(r["status"] == "OPTIMAL" for r in rows)
@@ -106,3 +114,15 @@ def test_failed_status_and_missing_clocks(tmp_path):
     assert float(rows[-2]["alg_time"]) == pytest.approx((1210 * 1010) ** 0.5 - 10, abs=1e-7)
     assert rows[-2]["process_time"] == ""
     assert rows[-1]["alg_time"] == "1"
+
+
+def test_legacy_qcqp_rows_do_not_stand(tmp_path):
+    """the reference's tests/test_dataset.py:17-26"""
+    path = tmp_path / "qc.mps"
+    path.write_text("NAME TEST\nQCMATRIX QC\n X X 0.5\nENDATA\n")
+    old = {"status": "OPTIMAL"}
+    assert not dataset.keep_previous(old, path)
+    old["input_format"] = dataset.INPUT_FORMAT
+    assert dataset.keep_previous(old, path)
+    old["status"] = "EXIT_1"
+    assert not dataset.keep_previous(old, path)

@@ -19,8 +19,8 @@ def _folder(tmp_path):
     for k in range(3):
         (data / f"qp{k}.mps").write_text(mps_cases.write_instance(instances.adjoint_case(k)))
     (data / "bad.mps").write_text(mps_cases.malformed()["bad_number"])
-    (data / "quad_rows.mps").write_text("NAME T\nROWS\n N obj\n L c1\nCOLUMNS\n    x obj 1 c1 1\nRHS\n"
-                                        "    rhs c1 1\nQCMATRIX c1\n    x x 1\nENDATA\n")
+    (data / "quad_rows.mps").write_text(mps_cases.random_qcqp_mps(3))  # second-order cones after the lift
+    (data / "nonconvex.mps").write_text(mps_cases.malformed_qcqp()["nonconvex_le"])
     return data
 
 
@@ -33,12 +33,16 @@ def test_dataset_runner_per_file_and_batched(engine_lib, tmp_path):
         assert dataset.main([str(data), str(out), "--stoptol", "1e-8"] + extra) == 0
         tables[mode] = {r["name"]: r for r in dataset.read_table(out / dataset.CSV_NAME)}
         lines = (out / dataset.CSV_NAME).read_text().splitlines()
-        assert lines[-2].startswith("SGM10,") and lines[-1].startswith("solved,,3,")
+        assert lines[-2].startswith("SGM10,") and lines[-1].startswith("solved,,4,")
         assert "qp0.mps" in (out / dataset.LOG_NAME).read_text()
     for mode, rows in tables.items():
-        assert sorted(rows) == ["bad.mps", "qp0.mps", "qp1.mps", "qp2.mps", "quad_rows.mps"]
-        assert rows["bad.mps"]["status"] == "INVALID_ARGUMENT"
-        assert rows["quad_rows.mps"]["status"] == "NOT_IMPLEMENTED"
+        assert sorted(rows) == ["bad.mps", "nonconvex.mps", "qp0.mps", "qp1.mps", "qp2.mps", "quad_rows.mps"]
+        assert rows["bad.mps"]["status"] == rows["nonconvex.mps"]["status"] == "INVALID_ARGUMENT"
+        assert rows["quad_rows.mps"]["status"] == "OPTIMAL" and rows["quad_rows.mps"]["row_cones"] == "4"
+        direct = hprqp.optimize(hprqp.read_from_mps(data / "quad_rows.mps"),
+                                hprqp.Parameters(verbose=False, stoptol=1e-8))
+        tol = 1e-6 * max(1.0, abs(direct.objective))
+        assert abs(float(rows["quad_rows.mps"]["primal_obj"]) - direct.objective) <= tol
         for k in range(3):
             r = rows[f"qp{k}.mps"]
             assert r["status"] == "OPTIMAL", (mode, r)

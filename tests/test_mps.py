@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from mps_cases import malformed, random_mps
+from mps_cases import malformed, malformed_qcqp, random_mps, random_qcqp_mps
 
 needs_ref = pytest.mark.skipif(not pyoracle.ref_available(), reason="reference CPU library not built")
 
@@ -26,9 +26,10 @@ def _ours(hprqp, path):
 
 
 def _same(a, b):
-    for k in ("n", "m", "obj_constant"):
+    for k in ("n", "m", "obj_constant", "num_var_cones", "num_row_cones"):
         assert a[k] == b[k], k
-    for k in ("q_indptr", "q_indices", "q_data", "a_indptr", "a_indices", "a_data", "c", "l", "u", "AL", "AU"):
+    for k in ("q_indptr", "q_indices", "q_data", "a_indptr", "a_indices", "a_data", "c", "l", "u", "AL", "AU",
+              "row_cone_offsets", "soc_rhs"):
         x, y = np.asarray(a[k]), np.asarray(b[k])
         assert x.shape == y.shape, k
         assert np.array_equal(x, y, equal_nan=True), k
@@ -101,3 +102,26 @@ def test_reference_fixture_model(engine_lib):
                       (got.A.indptr, "a_indptr"), (got.A.indices, "a_indices"), (got.A.data, "a_data"),
                       (got.c, "c"), (got.l, "l"), (got.u, "u"), (got.AL, "AL"), (got.AU, "AU")):
         assert np.array_equal(np.asarray(mine, float), np.asarray(ref[key], float)), key
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", range(6))
+def test_qcqp_models_identical_to_reference(engine_lib, tmp_path, seed):
+    """QCMATRIX rows lifted to second-order cones exactly as the reference's
+    reader and builder do (src/shared/mps_qp.cpp:119-206, qcqp.c)"""
+    p = tmp_path / f"qc{seed}.mps"
+    p.write_text(random_qcqp_mps(seed, n=8 + seed, m=6 + seed % 3))
+    ref = pyoracle.ref_build_from_mps(p)
+    assert ref["status"] == 0 and ref["num_row_cones"] == 4
+    ours = _ours(engine_lib, p)
+    assert ours["status"] == 0
+    _same(ours, ref)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", sorted(malformed_qcqp()))
+def test_qcqp_malformed_rejected_like_reference(engine_lib, tmp_path, name):
+    p = tmp_path / f"{name}.mps"
+    p.write_text(malformed_qcqp()[name])
+    assert pyoracle.ref_build_from_mps(p)["status"] != 0
+    assert _ours(engine_lib, p)["status"] != 0
