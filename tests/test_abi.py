@@ -128,3 +128,18 @@ def test_batch_rejects_bad_packing(engine_lib):
     p.var_offsets[-1] += 1  # does not end at n
     with pytest.raises(RuntimeError, match="INVALID_ARGUMENT"):
         batch.Batch(p)
+
+
+def test_reference_wrappers_find_every_symbol(engine_lib):
+    """every hprqp_* symbol the reference's Python and Julia packages bind
+    (tests/golden/reference_ffi_symbols.json, from
+    tests/golden/make_ffi_symbols.py) is exported, so both load this library
+    through HPRQP_LIBRARY_PATH unchanged"""
+    import ctypes
+    import json
+
+    lib = ctypes.CDLL(engine_lib.library_path())
+    data = json.loads((ROOT / "tests" / "golden" / "reference_ffi_symbols.json").read_text())
+    assert data["python"] and data["julia"]
+    missing = [s for names in data.values() for s in names if not hasattr(lib, s)]
+    assert not missing, missing
