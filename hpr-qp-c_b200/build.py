@@ -1,6 +1,12 @@
 """Build recipe of the engine library: nvcc, sm_100a only, in-tree.
 
     python hpr-qp-c_b200/build.py          # -> hpr-qp-c_b200/lib/libhprqp.so
+    python hpr-qp-c_b200/build.py --sanitize
+        # -> hpr-qp-c_b200/_build_san/libhprqp.so: the host code built with
+        #    AddressSanitizer + UndefinedBehaviorSanitizer (-O1 -g), for CPU
+        #    test runs of the builders, readers and bindings:
+        #    LD_PRELOAD="$(gcc -print-file-name=libasan.so) $(gcc -print-file-name=libubsan.so)"
+        #    ASAN_OPTIONS=detect_leaks=0 HPRQP_LIBRARY_PATH=<that .so> python -m pytest tests -m "not gpu"
 
 Compiles every source under csrc/ with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` into one shared
@@ -66,5 +72,28 @@ def build(verbose_ptxas: bool = False) -> Path:
     return LIB
 
 
+def build_sanitized() -> Path:
+    """Every source with host-side ASan + UBSan into _build_san/libhprqp.so
+    (always rebuilt; not used by the package unless HPRQP_LIBRARY_PATH
+    points at it)."""
+    out = PKG / "_build_san"
+    out.mkdir(parents=True, exist_ok=True)
+    flags = ["-Xcompiler", "-fPIC,-fsanitize=address,-fsanitize=undefined,-fno-omit-frame-pointer"]
+
+    def one(src: Path) -> Path:
+        obj = out / (src.name + ".o")
+        subprocess.run([nvcc(), *ARCH, "-O1", "-g", "-std=c++17", *flags, f"-I{INCLUDE}", f"-I{CSRC}", "-c",
+                        str(src), "-o", str(obj)], check=True)
+        return obj
+
+    srcs = _sources()
+    with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+        objs = list(ex.map(one, srcs))
+    lib = out / "libhprqp.so"
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lcudart", "-Xcompiler",
+                    "-fsanitize=address,-fsanitize=undefined"], check=True)
+    return lib
+
+
 if __name__ == "__main__":
-    print(build(verbose_ptxas="-v" in sys.argv))
+    print(build_sanitized() if "--sanitize" in sys.argv else build(verbose_ptxas="-v" in sys.argv))

@@ -168,8 +168,11 @@ class Batch:
         p = instances_or_packed if isinstance(instances_or_packed, Packed) else pack(instances_or_packed)
         self.packed = p
         keep = []
-        n = int(p.var_offsets[-1])
-        m = int(p.row_offsets[-1])
+        # matrix sizes from the arrays themselves (a C caller cannot be
+        # checked against array lengths): the library then rejects offsets
+        # that do not match them
+        n = len(p.q_indptr) - 1
+        m = len(p.a_indptr) - 1
         Q = _csr(n, n, p.q_indptr, p.q_indices, p.q_data, keep)
         A = _csr(m, n, p.a_indptr, p.a_indices, p.a_data, keep)
 

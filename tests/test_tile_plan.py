@@ -4,6 +4,7 @@ host-only probe compiled from the same header (tests/native)."""
 from __future__ import annotations
 
 import json
+import os
 import shutil
 import subprocess
 from pathlib import Path
@@ -21,14 +22,17 @@ def probe(tmp_path_factory):
     if not Path(nvcc).exists():
         pytest.skip("nvcc not available")
     exe = tmp_path_factory.mktemp("probe") / "tile_plan_probe"
+    # a clean environment: a sanitizer runtime preloaded into the test
+    # process must not reach nvcc or the probe
+    env = {k: v for k, v in os.environ.items() if k != "LD_PRELOAD"}
     subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17",
                     f"-I{ROOT / 'hpr-qp-c_b200' / 'csrc'}", f"-I{ROOT / 'include'}", "-o", str(exe),
-                    str(ROOT / "tests" / "native" / "tile_plan_probe.cu")], check=True)
+                    str(ROOT / "tests" / "native" / "tile_plan_probe.cu")], check=True, env=env)
 
     def run(indptr, indices):
         text = f"{len(indptr) - 1} {len(indices)}\n" + " ".join(map(str, indptr)) + "\n" + \
             " ".join(map(str, indices)) + "\n"
-        out = subprocess.run([str(exe)], input=text, capture_output=True, text=True, check=True).stdout
+        out = subprocess.run([str(exe)], input=text, capture_output=True, text=True, check=True, env=env).stdout
         return json.loads(out)
 
     return run
