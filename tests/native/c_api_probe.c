@@ -1,0 +1,38 @@
+/* A C caller of the host-side entry points (compiled as C11 by the CPU
+ * tests): the headers must be valid C, and the builders usable without a
+ * GPU.  Prints one JSON line. */
+#include <math.h>
+#include <stdio.h>
+
+#include "hprqp.h"
+#include "shared/build.h"
+#include "shared/qcqp.h"
+#include "shared/sparse.h"
+#include "shared/vector.h"
+
+int main(void)
+{
+    /* min x0^2 + x1^2 - x0  s.t.  x0 + x1 <= 1,  x0^2 + 2 x1^2 - 0.5 <= 0 */
+    size_t q_rp[] = {0, 1, 2}, q_ci[] = {0, 1}, a_rp[] = {0, 2}, a_ci[] = {0, 1};
+    double q_v[] = {2.0, 2.0}, a_v[] = {1.0, 1.0};
+    HPRQPMatrixCSR Q = {2, 2, 2, q_rp, q_ci, q_v, 0}, A = {1, 2, 2, a_rp, a_ci, a_v, 0};
+    double c[] = {-1.0, 0.0}, AL[] = {-INFINITY}, AU[] = {1.0}, l[] = {-INFINITY, -INFINITY}, u[] = {INFINITY, INFINITY};
+    size_t c_rp[] = {0, 0}, c_ci[] = {0}, d_rp[] = {0, 2}, d_ci[] = {0, 1};
+    double c_v[] = {0.0}, d_v[] = {2.0, 4.0}, constant[] = {-0.5};
+    HPRQPMatrixCSR C = {1, 2, 0, c_rp, c_ci, c_v, 0}, D = {1, 2, 2, d_rp, d_ci, d_v, 0};
+    HPRQPModel qp, qcqp;
+    model_init(&qp);
+    model_init(&qcqp);
+    HPRQPStatus s1 = build_from_QAbc(&Q, &A, c, AL, AU, l, u, 0.0, &qp);
+    HPRQPStatus s2 = build_from_QAbc_qc_diagonal(&Q, &A, c, AL, AU, l, u, 0.0, &C, constant, &D, &qcqp);
+    HPRQPStatus s3 = preprocess_model(&qp);
+    double y[1];
+    HPRQPStatus s4 = matrix_csr_matvec(&A, a_v, y);
+    printf("{\"build\": %d, \"qc\": %d, \"pre\": %d, \"matvec\": %d, \"y\": %g, \"m_qp\": %zu, \"m_qc\": %zu, "
+           "\"cones\": %zu, \"dot\": %g, \"soc\": %d}\n",
+           (int)s1, (int)s2, (int)s3, (int)s4, y[0], qp.A.nrow, qcqp.A.nrow, qcqp.num_row_cones,
+           vec_dot(a_v, a_v, 2), (int)model_validate_soc(&qcqp));
+    model_free(&qp);
+    model_free(&qcqp);
+    return 0;
+}
