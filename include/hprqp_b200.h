@@ -1,8 +1,8 @@
 /*
  * hprqp_b200.h -- engine diagnostics used by the parity tests and the
  * benchmark.  These have no counterpart in the reference's public API; the
- * reference exposes the same quantities only through internal headers
- * (include/gpu/*.h) to its own C tests.
+ * reference exposes the same quantities only through the internal headers
+ * of its include/gpu directory to its own C tests.
  */
 #ifndef HPRQP_B200_H
 #define HPRQP_B200_H

@@ -4,7 +4,12 @@
 #include <math.h>
 #include <stdio.h>
 
+#include "gpu/gpu.h"
 #include "hprqp.h"
+#include "hprqp_b200.h"
+#include "hprqp_batch.h"
+#include "hprqp_binding.h"
+#include "hprqp_diff.h"
 #include "shared/build.h"
 #include "shared/qcqp.h"
 #include "shared/sparse.h"
@@ -28,10 +33,26 @@ int main(void)
     HPRQPStatus s3 = preprocess_model(&qp);
     double y[1];
     HPRQPStatus s4 = matrix_csr_matvec(&A, a_v, y);
+    /* the binding ABI, as the reference's tests/test_binding_api.c drives it;
+       without a GPU the solve fails loudly */
+    HPRQPBindingModel *bm = NULL;
+    HPRQPBindingParams *bp = NULL;
+    HPRQPBindingResults *br = NULL;
+    int bind = hprqp_model_create(&bm) | hprqp_params_create(&bp) | hprqp_results_create(&br);
+    bind |= hprqp_model_build_from_qabc_csr(bm, 2, 2, 2, q_rp, q_ci, q_v, 1, 2, 2, a_rp, a_ci, a_v, c, AL, AU, l,
+                                            u, 0.0);
+    bind |= hprqp_params_set_verbose(bp, 0);
+    size_t bn = hprqp_model_num_variables(bm), bmr = hprqp_model_num_constraints(bm);
+    int solve = (int)hprqp_optimize(bm, bp, br);
+    hprqp_results_destroy(br);
+    hprqp_params_destroy(bp);
+    hprqp_model_destroy(bm);
     printf("{\"build\": %d, \"qc\": %d, \"pre\": %d, \"matvec\": %d, \"y\": %g, \"m_qp\": %zu, \"m_qc\": %zu, "
-           "\"cones\": %zu, \"dot\": %g, \"soc\": %d}\n",
+           "\"cones\": %zu, \"dot\": %g, \"soc\": %d, \"bind\": %d, \"bn\": %zu, \"bm\": %zu, "
+           "\"solve\": %d, \"gpu\": %d}\n",
            (int)s1, (int)s2, (int)s3, (int)s4, y[0], qp.A.nrow, qcqp.A.nrow, qcqp.num_row_cones,
-           vec_dot(a_v, a_v, 2), (int)model_validate_soc(&qcqp));
+           vec_dot(a_v, a_v, 2), (int)model_validate_soc(&qcqp), bind, bn, bmr, solve,
+           gpu_backend_available());
     model_free(&qp);
     model_free(&qcqp);
     return 0;

@@ -29,3 +29,6 @@ def test_c_caller(engine_lib, tmp_path):
     assert out["y"] == 2.0 and out["dot"] == 2.0
     # one linear row, then one cone: 2 head rows + 2 factor rows
     assert out["m_qp"] == 1 and out["m_qc"] == 1 + 4 and out["cones"] == 1
+    assert out["bind"] == 0 and (out["bn"], out["bm"]) == (2, 1)
+    if not out["gpu"]:
+        assert out["solve"] == engine_lib.STATUS_NOT_IMPLEMENTED  # no CPU fallback
