@@ -1,5 +1,5 @@
-/* A C caller of the host-side entry points (compiled as C11 by the CPU
- * tests): the headers must be valid C, and the builders usable without a
+/* A C caller of the host-side entry points (compiled as pedantic C99 by the
+ * CPU tests): the headers must be valid C, and the builders usable without a
  * GPU.  Prints one JSON line. */
 #include <math.h>
 #include <stdio.h>

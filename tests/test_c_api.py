@@ -1,5 +1,5 @@
 """The host-side C entry points from a C program (tests/native/c_api_probe.c,
-compiled as C11 against include/ and linked to the library): the headers are
+compiled as pedantic C99 against include/ and linked to the library): the headers are
 valid C and the builders work without a GPU."""
 from __future__ import annotations
 
@@ -21,7 +21,7 @@ def test_c_caller(engine_lib, tmp_path):
     lib = Path(engine_lib.library_path())
     exe = tmp_path / "c_api_probe"
     env = {k: v for k, v in os.environ.items() if k != "LD_PRELOAD"}
-    subprocess.run([cc, "-std=c11", "-Wall", "-Werror", f"-I{ROOT / 'include'}", "-o", str(exe),
+    subprocess.run([cc, "-std=c99", "-pedantic", "-Wall", "-Wextra", "-Werror", f"-I{ROOT / 'include'}", "-o", str(exe),
                     str(ROOT / "tests" / "native" / "c_api_probe.c"), f"-L{lib.parent}", f"-l:{lib.name}",
                     f"-Wl,-rpath,{lib.parent}", "-lm"], check=True, env=env)
     out = json.loads(subprocess.run([str(exe)], capture_output=True, text=True, check=True, env=env).stdout)
