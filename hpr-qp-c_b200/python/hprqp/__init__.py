@@ -460,6 +460,62 @@ def build_from_qabc_soc(Q, c, A, AL, AU, l, u, var_cone_offsets=None, row_cone_o
     return model
 
 
+def build_from_qabc_qc(Q, c, A, AL, AU, l, u, C, constant, R=None, offsets=None, D=None,
+                       obj_constant: float = 0.0) -> Model:
+    """QP with convex quadratic constraints (include/shared/qcqp.h):
+    row i of C with constant[i] and either the factor R_i (rows
+    [offsets[i], offsets[i+1]) of R: build_from_QAbc_qc_factors) or the
+    diagonal D_i (row i of D: build_from_QAbc_qc_diagonal) gives
+    C_i x + 1/2 |R_i x|^2 + constant_i <= 0  (D_i = R_i' R_i).  Each is
+    lifted to one second-order cone after the rows of A; solve_gpu runs the
+    cone path.  The matrices may be dense or scipy sparse."""
+    if (R is None) == (D is None):
+        raise ValueError("give either R with offsets or D")
+    keep = []
+
+    def csr(mat):
+        nr, nc, p, i, v = _matrix_to_csr(mat)
+        p = np.ascontiguousarray(p if len(p) else np.zeros(1), np.uint64)
+        i = np.ascontiguousarray(i if len(i) else np.zeros(1), np.uint64)
+        v = np.ascontiguousarray(v if len(v) else np.zeros(1), np.float64)
+        keep.extend([p, i, v])
+        return _MatrixCSR(nr, nc, int(p[-1]), p.ctypes.data_as(c_size_p), i.ctypes.data_as(c_size_p),
+                          v.ctypes.data_as(c_double_p), 0)
+
+    def db(a, k, name):
+        arr = _vec(a, k, name) if k else np.zeros(1)
+        keep.append(arr)
+        return arr.ctypes.data_as(c_double_p)
+
+    Qc, Cc = csr(Q), csr(C)
+    n = int(Qc.ncol)
+    Ac = csr(A)
+    if Ac.nrow == 0:
+        Ac.ncol = n
+    m, nq = int(Ac.nrow), int(Cc.nrow)
+    lib = _lib()
+    M = ctypes.POINTER(_MatrixCSR)
+    head = [ctypes.byref(Qc), ctypes.byref(Ac), db(c, n, "c"), db(AL, m, "AL") if m else None,
+            db(AU, m, "AU") if m else None, db(l, n, "l"), db(u, n, "u"), float(obj_constant), ctypes.byref(Cc),
+            db(constant, nq, "constant")]
+    model = Model()
+    if D is not None:
+        fn = lib.build_from_QAbc_qc_diagonal
+        fn.argtypes = [M, M] + [c_double_p] * 5 + [ctypes.c_double, M, c_double_p, M, ctypes.c_void_p]
+        args = head + [ctypes.byref(csr(D)), model._handle]
+    else:
+        off = np.ascontiguousarray(np.asarray(offsets if offsets is not None else [], np.uint64))
+        if off.shape[0] != nq + 1:
+            raise ValueError(f"offsets: expected {nq + 1} entries, got {off.shape[0]}")
+        keep.append(off)
+        fn = lib.build_from_QAbc_qc_factors
+        fn.argtypes = [M, M] + [c_double_p] * 5 + [ctypes.c_double, M, c_double_p, M, c_size_p, ctypes.c_void_p]
+        args = head + [ctypes.byref(csr(R)), off.ctypes.data_as(c_size_p), model._handle]
+    fn.restype = ctypes.c_int
+    _raise_for_status(fn(*args), "build_from_QAbc_qc")
+    return model
+
+
 def build_from_instance(inst) -> Model:
     """Model from an ``instances.QPInstance`` (CSR arrays, no copies in Python)."""
     return build_from_qabc(inst.Q, inst.c, inst.A, inst.AL, inst.AU, inst.l, inst.u, inst.obj_constant)
@@ -735,5 +791,5 @@ __all__ = [
     "STATUS_ALLOCATION_FAILED", "STATUS_CONTINUE", "STATUS_INVALID_ARGUMENT", "STATUS_MAX_ITER",
     "STATUS_NOT_IMPLEMENTED", "STATUS_OK", "STATUS_OPTIMAL", "STATUS_TIME_LIMIT", "build_from_mps",
     "build_from_QAbc", "build_from_qabc", "build_from_qabc_soc", "build_from_instance", "gpu_backend_available", "optimize",
-    "read_from_mps", "status_name", "spmv", "setup_info", "model_arrays", "launch_count", "library_path",
+    "read_from_mps", "status_name", "spmv", "build_from_qabc_qc", "setup_info", "model_arrays", "launch_count", "library_path",
 ]
