@@ -1,0 +1,34 @@
+"""bench.py --impl reference on CPU (it runs the reference's own CPU build,
+oracle/_ref, on a bounded sample): one JSON line with the contract's keys,
+the metric and config of the GPU arm, impl "reference", a cpu_baseline
+describing the run and an e2e block with zero transfer bytes."""
+from __future__ import annotations
+
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+import pyoracle
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="reference CPU library not built")
+def test_reference_arm_json_line():
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup",
+                          "0", "--cpu-sample", "8"], capture_output=True, text=True, timeout=600, check=True,
+                         cwd=ROOT).stdout
+    lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+                "vs_baseline", "dtype", "data", "config"):
+        assert key in d, key
+    assert d["impl"] == "reference" and d["unit"] == "solves/s" and d["value"] > 0 and d["higher_is_better"]
+    assert d["config"]["global_batch"] == 4096 and d["n_gpus"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and "sample" in cb
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
