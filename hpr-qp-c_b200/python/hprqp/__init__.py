@@ -791,5 +791,5 @@ __all__ = [
     "STATUS_ALLOCATION_FAILED", "STATUS_CONTINUE", "STATUS_INVALID_ARGUMENT", "STATUS_MAX_ITER",
     "STATUS_NOT_IMPLEMENTED", "STATUS_OK", "STATUS_OPTIMAL", "STATUS_TIME_LIMIT", "build_from_mps",
     "build_from_QAbc", "build_from_qabc", "build_from_qabc_soc", "build_from_instance", "gpu_backend_available", "optimize",
-    "read_from_mps", "status_name", "spmv", "build_from_qabc_qc", "setup_info", "model_arrays", "launch_count", "library_path",
+    "read_from_mps", "status_name", "spmv", "gather_bound", "build_from_qabc_qc", "setup_info", "model_arrays", "launch_count", "library_path",
 ]
