@@ -69,13 +69,27 @@ class ClockSampler:
 
     def __init__(self, device: int):
         self.device = device
+        self.smi_id = self.physical_id(device)
         self.proc = None
         self.path = Path("/tmp") / f"hprqp_clocks_{os.getpid()}.csv"
+
+    @staticmethod
+    def physical_id(device: int, visible: str | None = None) -> str:
+        """nvidia-smi's id of CUDA device `device`: CUDA_VISIBLE_DEVICES
+        renumbers devices (its entries are indices or UUIDs, both of which
+        nvidia-smi --id takes); without it the CUDA index is the physical one."""
+        if visible is None:
+            visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if visible:
+            ids = [v.strip() for v in visible.split(",") if v.strip()]
+            if 0 <= device < len(ids):
+                return ids[device]
+        return str(device)
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                ["nvidia-smi", f"--id={self.smi_id}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None

@@ -6,8 +6,9 @@
  * and meaning:
  *   model_init / model_free / model_copy      hprqp.h:14-16 (src/shared/build.c:402-502)
  *   build_from_QAbc                           hprqp.h:17-24 (src/shared/build.c:608-621)
- *   build_from_QAbc_soc                       hprqp.h:26-30 (cones: NOT_IMPLEMENTED here)
- *   build_from_mps                            hprqp.h:31    (MPS input: NOT_IMPLEMENTED here)
+ *   build_from_QAbc_soc                       hprqp.h:26-30 (src/shared/build.c:39-99, second-order cones)
+ *   build_from_mps                            hprqp.h:31    (src/shared/mps_qp.cpp:208-326, free-format MPS
+ *                                                            with QUADOBJ/QMATRIX and diagonal QCMATRIX rows)
  *   params_set_defaults / results_init/free   hprqp.h:33-35 (src/shared/solver.c:133-177)
  *   print_model_info / print_params_info      hprqp.h:36-37 (src/shared/solver_backend.c:240-271)
  *   solve_gpu                                 hprqp.h:38    (src/gpu/solver.cu:127-232)
@@ -19,7 +20,10 @@
  *   - CPU polishing and the equality-Gram metric do not exist; their
  *     parameters are accepted and ignored (the reference with
  *     --polishing 0 --gram off);
- *   - second-order cones and MPS input return HPRQP_STATUS_NOT_IMPLEMENTED.
+ *   - second-order cones (build_from_QAbc_soc), MPS input (build_from_mps)
+ *     and convex quadratic constraints (include/shared/qcqp.h, lifted to
+ *     rotated Lorentz cones) are supported by solve_gpu; the batch API and
+ *     the adjoints (hprqp_batch.h, hprqp_diff.h) take QPs without cones.
  */
 #ifndef HPRQP_H
 #define HPRQP_H

@@ -28,7 +28,8 @@ int hprqp_gpu_backend_available(void);
 
 HPRQPStatus hprqp_model_create(HPRQPBindingModel **out_model);
 void hprqp_model_destroy(HPRQPBindingModel *model);
-/* MPS input is outside this engine: returns HPRQP_STATUS_NOT_IMPLEMENTED. */
+/* Reads a free-format MPS file (QUADOBJ/QMATRIX, diagonal QCMATRIX rows)
+ * into the model, as build_from_mps does. */
 HPRQPStatus hprqp_model_read_from_mps(HPRQPBindingModel *model, const char *mps_path);
 HPRQPStatus hprqp_model_build_from_qabc_csr(HPRQPBindingModel *model,
                                             size_t q_nrow,

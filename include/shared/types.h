@@ -8,10 +8,11 @@
  * order, field types and enum numbering are therefore fixed; the comments are
  * this project's own.
  *
- * Fields that belong to subsystems this engine does not implement (second
- * order cones, the equality Gram metric, CPU polishing) keep their slots so
- * the layout stays the same; the engine ignores them or rejects non-empty
- * cone data with HPRQP_STATUS_NOT_IMPLEMENTED.
+ * Fields that belong to subsystems this engine does not implement (the
+ * equality Gram metric, CPU polishing) keep their slots so the layout stays
+ * the same; the engine ignores them.  Second-order cones are supported by
+ * solve_gpu (build_from_QAbc_soc, and QCQP rows lifted to cones); the batch
+ * API and the adjoints reject models with cones.
  */
 #ifndef HPRQP_TYPES_H
 #define HPRQP_TYPES_H
@@ -55,8 +56,9 @@ typedef struct HPRQPMatrixCSR {
     int owns_data;
 } HPRQPMatrixCSR;
 
-/* Second-order-cone description (kept for ABI; cones are not supported by
- * this engine).  Reference: types.h:37-48. */
+/* Second-order-cone description: the last variables and the last rows of a
+ * model may form Lorentz cones (offsets of each cone's first entry).
+ * Reference: types.h:37-48. */
 typedef struct HPRQPSOCSpec {
     size_t num_var_cones;
     const size_t *var_offsets;

@@ -8,7 +8,7 @@ caps and tolerances, and records what it returns.  The fixtures pin the
 oracle (tests/test_oracle_golden.py) without needing the reference at test
 time.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF_ROOT=<reference checkout> && python tests/golden/make_golden.py
 """
 from __future__ import annotations
 

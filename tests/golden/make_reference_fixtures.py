@@ -4,7 +4,7 @@ of it: its reader's model arrays (its CPU library's build_from_mps) and its
 CPU solver's result at max_iter 0 and at stoptol 1e-8.  Writes simple_qp.mps
 and simple_qp.json beside this file.
 
-    make -C oracle ref && python tests/golden/make_reference_fixtures.py <reference checkout>
+    make -C oracle ref REF_ROOT=<reference checkout> && python tests/golden/make_reference_fixtures.py <reference checkout>
 """
 from __future__ import annotations
 

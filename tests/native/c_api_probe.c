@@ -15,8 +15,9 @@
 #include "shared/sparse.h"
 #include "shared/vector.h"
 
-int main(void)
+int main(int argc, char **argv)
 {
+    /* argv[1]: an MPS file for build_from_mps (optional) */
     /* min x0^2 + x1^2 - x0  s.t.  x0 + x1 <= 1,  x0^2 + 2 x1^2 - 0.5 <= 0 */
     size_t q_rp[] = {0, 1, 2}, q_ci[] = {0, 1}, a_rp[] = {0, 2}, a_ci[] = {0, 1};
     double q_v[] = {2.0, 2.0}, a_v[] = {1.0, 1.0};
@@ -33,6 +34,23 @@ int main(void)
     HPRQPStatus s3 = preprocess_model(&qp);
     double y[1];
     HPRQPStatus s4 = matrix_csr_matvec(&A, a_v, y);
+    /* second-order cones: (x0, x1) in a 2-dimensional Lorentz cone, and the
+       one row as a row cone of size 1 with rhs 0 (offsets end at n and m;
+       cone variables and cone rows are unbounded) */
+    size_t var_off[] = {0, 2}, row_off[] = {0, 1};
+    double rhs[] = {0.0};
+    HPRQPSOCSpec soc = {1, var_off, 1, row_off, rhs};
+    HPRQPModel socm, mps;
+    model_init(&socm);
+    model_init(&mps);
+    double ALs[] = {-INFINITY}, AUs[] = {INFINITY};
+    HPRQPStatus s5 = build_from_QAbc_soc(&Q, &A, c, ALs, AUs, l, u, 0.0, &soc, &socm);
+    HPRQPStatus s6 = argc > 1 ? build_from_mps(argv[1], &mps) : HPRQP_STATUS_INVALID_ARGUMENT;
+    HPRQPBindingModel *mb = NULL;
+    int bind_mps = argc > 1 ? (int)hprqp_model_create(&mb) : -1;
+    if (argc > 1 && bind_mps == 0) bind_mps = (int)hprqp_model_read_from_mps(mb, argv[1]);
+    size_t mps_n_bind = mb ? hprqp_model_num_variables(mb) : 0;
+    hprqp_model_destroy(mb);
     /* the binding ABI, as the reference's tests/test_binding_api.c drives it;
        without a GPU the solve fails loudly */
     HPRQPBindingModel *bm = NULL;
@@ -49,10 +67,15 @@ int main(void)
     hprqp_model_destroy(bm);
     printf("{\"build\": %d, \"qc\": %d, \"pre\": %d, \"matvec\": %d, \"y\": %g, \"m_qp\": %zu, \"m_qc\": %zu, "
            "\"cones\": %zu, \"dot\": %g, \"soc\": %d, \"bind\": %d, \"bn\": %zu, \"bm\": %zu, "
-           "\"solve\": %d, \"gpu\": %d}\n",
+           "\"solve\": %d, \"gpu\": %d, \"soc_build\": %d, \"soc_var_cones\": %zu, \"soc_row_cones\": %zu, "
+           "\"mps\": %d, \"mps_n\": %zu, \"mps_m\": %zu, \"mps_nnz_q\": %zu, \"bind_mps\": %d, "
+           "\"bind_mps_n\": %zu}\n",
            (int)s1, (int)s2, (int)s3, (int)s4, y[0], qp.A.nrow, qcqp.A.nrow, qcqp.num_row_cones,
            vec_dot(a_v, a_v, 2), (int)model_validate_soc(&qcqp), bind, bn, bmr, solve,
-           gpu_backend_available());
+           gpu_backend_available(), (int)s5, socm.num_var_cones, socm.num_row_cones, (int)s6, mps.Q.ncol,
+           mps.A.nrow, mps.Q.nnz, bind_mps, mps_n_bind);
+    model_free(&socm);
+    model_free(&mps);
     model_free(&qp);
     model_free(&qcqp);
     return 0;

@@ -67,3 +67,16 @@ def test_single_rank_is_identity():
     assert bench.max_over_ranks(3.5, None) == 3.5
     assert bench.rank_first_instance(0) == 0
     assert bench.whole_job_rate(10, 1, 2, 4.0) == 5.0
+
+
+def test_clock_sampler_maps_visible_devices():
+    """Under torchrun each rank's CUDA device 0..N-1 is renumbered by
+    CUDA_VISIBLE_DEVICES; the clock samples must come from that physical GPU."""
+    sys.path[:0] = [str(ROOT)]
+    import bench
+
+    pid = bench.ClockSampler.physical_id
+    assert pid(1, "") == "1"
+    assert pid(0, "3,5") == "3" and pid(1, "3,5") == "5"
+    assert pid(0, "GPU-8f3a, GPU-11b2") == "GPU-8f3a" and pid(1, "GPU-8f3a, GPU-11b2") == "GPU-11b2"
+    assert pid(4, "3,5") == "4"  # out of range: leave the index alone
