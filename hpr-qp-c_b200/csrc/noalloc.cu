@@ -20,11 +20,20 @@
 //
 // Host code cannot use the array's name as a device address (it denotes a
 // host-side shadow), so the first call on each device, with that device
-// current, looks up the real address with cudaGetSymbolAddress and caches it;
-// make that first call before any stream capture on the device.
+// current, looks up the real address with cudaGetSymbolAddress and caches it
+// together with the identity of the device's current CUDA context
+// (cuCtxGetId).  A later call that finds another context on the device -- the
+// caller ran cudaDeviceReset, or the primary context was released and created
+// again, which reloads the module at a new address -- looks the address up
+// again instead of using a stale one.  Make the first call on a device before
+// any stream capture there: it may load this library's device code.
+//
+// The call selects `device` for its own work and restores the caller's
+// current device before it returns, on every path.
 #include "hprqp_b200.h"
 #include "rowblock.cuh"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -41,7 +50,12 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-static double *g_scratch_addr[kMaxDevices];
+struct ScratchSlot {
+    double *addr;
+    unsigned long long ctx_id;  // cuCtxGetId of the context the address belongs to
+    bool has_id;
+};
+static ScratchSlot g_scratch_slot[kMaxDevices];
 static std::mutex g_scratch_mutex;
 
 static __global__ void k_probe(double *z, int len)
@@ -153,11 +167,45 @@ static int grid_for(long long work)
     return (int)(g < 1 ? 1 : (g > kMaxBlocks ? kMaxBlocks : g));
 }
 
-// address of the scratch array on `device` (looked up once per device)
+// Identity of the current context (cuCtxGetId, reached through the runtime's
+// driver entry points so the library links only cudart); false when the
+// driver does not offer it.
+static bool current_context_id(unsigned long long *id)
+{
+    using GetCurrentFn = CUresult (*)(CUcontext *);
+    using GetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void *f0 = nullptr, *f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0, q1;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) == cudaSuccess &&
+            q0 == cudaDriverEntryPointSuccess && cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) ==
+                                                     cudaSuccess && q1 == cudaDriverEntryPointSuccess) {
+            get_current = (GetCurrentFn)f0;
+            get_id = (GetIdFn)f1;
+        }
+        cudaGetLastError();  // a missing entry point is not an error of this call
+        looked_up = true;
+    }
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Address of the scratch array on `device`, which must be current: looked up
+// on the first call in each context of the device and cached with that
+// context's id.  Without context ids (an old driver) it is looked up on
+// every call.
 static HPRQPStatus scratch_for(int device, double **out)
 {
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[device]) {
+    ScratchSlot &slot = g_scratch_slot[device];
+    unsigned long long id = 0;
+    const bool has_id = current_context_id(&id);
+    if (!slot.addr || !has_id || !slot.has_id || slot.ctx_id != id) {
         double *ptr = nullptr;
         const cudaError_t err = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
         if (err != cudaSuccess || ptr == nullptr) {
@@ -165,11 +213,30 @@ static HPRQPStatus scratch_for(int device, double **out)
                     cudaGetErrorString(err));
             return HPRQP_STATUS_NOT_IMPLEMENTED;
         }
-        g_scratch_addr[device] = ptr;
+        slot.addr = ptr;
+        slot.ctx_id = id;
+        slot.has_id = has_id;
     }
-    *out = g_scratch_addr[device];
+    *out = slot.addr;
     return HPRQP_STATUS_OK;
 }
+
+// Makes `device` current for the duration of a call and gives the caller's
+// current device back on every return path.
+class DeviceGuard {
+public:
+    DeviceGuard() { ok_ = cudaGetDevice(&saved_) == cudaSuccess; }
+    ~DeviceGuard()
+    {
+        if (ok_) cudaSetDevice(saved_);
+    }
+    DeviceGuard(const DeviceGuard &) = delete;
+    DeviceGuard &operator=(const DeviceGuard &) = delete;
+
+private:
+    int saved_ = 0;
+    bool ok_ = false;
+};
 
 #define NA_CK(call)                                                                                   \
     do {                                                                                              \
@@ -194,7 +261,17 @@ static HPRQPStatus power_lambda(int device, size_t m, size_t n, const int *a_rp,
 {
     if (!lambda_out || (m > 0 && (!a_rp || !a_ci || !a_v || !at_rp || !at_ci || !at_v)))
         return HPRQP_STATUS_INVALID_ARGUMENT;
-    if (device < 0 || device >= kMaxDevices) return HPRQP_STATUS_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess) {
+        cudaGetLastError();
+        fprintf(stderr, "hprqp-b200: no CUDA device available; this engine has no CPU fallback\n");
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
+    }
+    if (device < 0 || device >= ndev || device >= kMaxDevices) {
+        fprintf(stderr, "hprqp-b200: hprqp_b200_power_lambda_noalloc: device %d does not exist (%d visible)\n",
+                device, ndev);
+        return HPRQP_STATUS_INVALID_ARGUMENT;
+    }
     if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || 2 * m + n > kNoAllocDoubles - kPartSlots) {
         fprintf(stderr,
                 "hprqp-b200: hprqp_b200_power_lambda_noalloc: 2*m + n = %zu exceeds the fixed scratch of %zu "
@@ -205,6 +282,7 @@ static HPRQPStatus power_lambda(int device, size_t m, size_t n, const int *a_rp,
     *lambda_out = 0.0;
     if (iterations_out) *iterations_out = 0;
     if (m == 0) return HPRQP_STATUS_OK;
+    DeviceGuard restore_device;
     NA_CK(cudaSetDevice(device));
     double *base = nullptr;
     HPRQPStatus st = scratch_for(device, &base);

@@ -77,12 +77,26 @@ HPRQPStatus hprqp_b200_setup(const HPRQPModel *model, const HPRQPParams *params,
  * HPRQP_STATUS_INVALID_ARGUMENT).  The array is shared by all calls and
  * keeps the previous call's contents, so calls on the same device must not
  * overlap in time.  The first call on a device looks up the array's device
- * address; make it before any stream capture on that device.  Nothing is
- * allocated: no cudaMalloc, no cudaFree, no allocating library call. */
+ * address (again after a cudaDeviceReset or a new primary context); make it
+ * before any stream capture on that device.  `device` must be a visible
+ * device (else HPRQP_STATUS_INVALID_ARGUMENT); the caller's current device is
+ * restored before the call returns.  Nothing is allocated: no cudaMalloc, no
+ * cudaFree, no allocating library call (the 8 MiB array is reserved when the
+ * library's device code is loaded on the device, not by a call). */
 HPRQPStatus hprqp_b200_power_lambda_noalloc(int device, size_t m, size_t n, const int *a_row_ptr,
                                             const int *a_col, const double *a_val, const int *at_row_ptr,
                                             const int *at_col, const double *at_val, void *stream,
                                             double *lambda_out, int *iterations_out);
+
+/* Routing of solve_gpu (an addition: the reference runs every model through
+ * its host-driven loop, src/shared/solver_backend.c:432-513).  A model
+ * without cones whose products per iteration touch at most max_work
+ * nonzeros (2 nnz(Q) + 2 nnz(A)) is solved in one CTA of the batch kernel
+ * -- same method, same results up to rounding, one launch instead of host
+ * round trips per iteration -- unless it is solved for the adjoint
+ * (hprqp_solve_for_backward).  max_work = 0 sends every model through the
+ * host-driven loop.  Process-wide; returns the previous value. */
+size_t hprqp_b200_set_single_cta_max_work(size_t max_work);
 
 /* Number of engine kernel launches issued by this process so far
  * (graph replays count each captured kernel). */
