@@ -173,15 +173,15 @@ def _ref_worker(args):
     inst_ids, stoptol = args
     import pyoracle
 
-    statuses = []
+    out = []
     for k in inst_ids:
         inst = batch_instances(1, k)[0]
         if pyoracle.ref_available():
             r = pyoracle.ref_solve(inst, stoptol=stoptol)
         else:
             r = pyoracle.OracleModel(inst).solve(stoptol=stoptol, mode=pyoracle.MODE_CPU_REF)
-        statuses.append(int(r["status"]))
-    return statuses
+        out.append((int(k), int(r["status"]), float(r["primal_obj"])))
+    return out
 
 
 def _ref_single_core(_):
@@ -225,18 +225,109 @@ def cpu_reference_rate(ids, cores: int):
     with ctx.Pool(cores) as pool:
         pool.map(int, range(cores))  # start the workers outside the timed region
         t0 = time.perf_counter()
-        statuses = sum(pool.map(_ref_worker, [(c, STOPTOL) for c in chunks if c]), [])
+        solved = sum(pool.map(_ref_worker, [(c, STOPTOL) for c in chunks if c]), [])
         dt = time.perf_counter() - t0
-    return len(ids) / dt, kind, dt, statuses
+    # (instance id, status, primal objective), in instance order
+    return len(ids) / dt, kind, dt, sorted(solved)
 
 
-def spmv_leg(peak_gbs: float, reps: int = 10):
+def objective_agreement(ours_status, ours_obj, ref_solved):
+    """The batch's objectives against the reference CPU solves of the same
+    instances: both OPTIMAL, largest |ours - ref| / max(1, |ref|)."""
+    diffs, both = [], 0
+    for k, st, obj in ref_solved:
+        if st == 6 and int(ours_status[k]) == 6:
+            both += 1
+            diffs.append(abs(float(ours_obj[k]) - obj) / max(1.0, abs(obj)))
+    return {"instances": len(ref_solved), "both_optimal": both,
+            "max_rel_objective_diff": float(max(diffs)) if diffs else None}
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_gpu_leg(device: int, sample: int = 32, large_iters: int = 1000):
+    """The reference's own GPU solve_gpu (its CUDA build: cuSPARSE SpMV and
+    cuBLAS reductions, polishing 0, Gram off) beside this engine's solve_gpu
+    on the same seeded instances and the same GPU: the n=1000 QP, a sample
+    of the batch recipe (and the batched kernel on it), the portfolio QP and
+    the large power-law QP at a fixed iteration budget.  A baseline, like
+    cpu_baseline: the reference measured, never this engine."""
+    import hprqp
+    import pyoracle
+    from hprqp import batch as hb
+    from hprqp import instances
+
+    if not pyoracle.ref_gpu_available():
+        return {"unavailable": "the reference GPU library (oracle/_ref/libhprqp_ref_gpu.so) is not built"}
+
+    def ours(inst, stoptol, max_iter=2147483647, model=None):
+        model = model or hprqp.build_from_instance(inst)
+        t0 = time.perf_counter()
+        r = hprqp.optimize(model, hprqp.Parameters(verbose=False, stoptol=stoptol, max_iter=max_iter,
+                                                   device_number=device), as_numpy=True)
+        return {"status": r.status_code, "iter": int(r.iter), "loop_s": r.time,
+                "call_s": time.perf_counter() - t0, "objective": r.objective}
+
+    def ref(inst, stoptol, max_iter=2147483647, model=None):
+        model = model or pyoracle.RefGpuModel(inst)
+        t0 = time.perf_counter()
+        o = model.solve(stoptol=stoptol, max_iter=max_iter, device=device)
+        return {"status": int(o["status"]), "iter": int(o["iter"]), "loop_s": float(o["time"]),
+                "call_s": time.perf_counter() - t0, "objective": float(o["primal_obj"])}
+
+    def pair(name, inst, stoptol, max_iter=2147483647):
+        om, rm = hprqp.build_from_instance(inst), pyoracle.RefGpuModel(inst)
+        ours(inst, stoptol, 10, om)  # load both libraries' kernels outside the timings
+        ref(inst, stoptol, 10, rm)
+        a, b = ours(inst, stoptol, max_iter, om), ref(inst, stoptol, max_iter, rm)
+        return {"workload": name, "stoptol": stoptol, "ours": a, "reference_gpu": b,
+                "iters_per_s": {"ours": a["iter"] / a["loop_s"], "reference_gpu": b["iter"] / b["loop_s"]},
+                "loop_speedup": (b["loop_s"] / b["iter"]) / (a["loop_s"] / a["iter"]),
+                "call_speedup": b["call_s"] / a["call_s"],
+                "rel_objective_diff": abs(a["objective"] - b["objective"]) / max(1.0, abs(b["objective"]))}
+
+    out = {"plain_qp_n1000": pair("plain QP n=1000 m=500 (1% A density)", instances.config0(), 1e-6)}
+    insts = batch_instances(sample, 0)
+    om = [hprqp.build_from_instance(i) for i in insts]
+    rm = [pyoracle.RefGpuModel(i) for i in insts]
+    ours(insts[0], STOPTOL, 10, om[0])
+    ref(insts[0], STOPTOL, 10, rm[0])
+    ra = [ours(i, STOPTOL, model=m) for i, m in zip(insts, om)]
+    rb = [ref(i, STOPTOL, model=m) for i, m in zip(insts, rm)]
+    b = hb.Batch(insts, device_number=device)
+    b.solve(stoptol=STOPTOL)
+    bms = b.solve(stoptol=STOPTOL)
+    b.close()
+    ta, tb = sum(x["call_s"] for x in ra), sum(x["call_s"] for x in rb)
+    out["batch_sample"] = {
+        "workload": f"{sample} instances of the batch recipe, stoptol {STOPTOL:g}, one solve_gpu call each",
+        "solves_per_s": {"ours_plain": sample / ta, "reference_gpu_plain": sample / tb,
+                         "ours_batched": sample / (bms / 1e3)},
+        "plain_speedup": tb / ta,
+        "optimal": {"ours": sum(x["status"] == 6 for x in ra), "reference_gpu": sum(x["status"] == 6 for x in rb)},
+        "max_rel_objective_diff": max(abs(x["objective"] - y["objective"]) / max(1.0, abs(y["objective"]))
+                                      for x, y in zip(ra, rb))}
+    out["portfolio"] = pair("portfolio n=200,200 (k=200 factors, 500 sectors)", instances.config2(), 1e-6)
+    out["large_qp"] = pair(f"power-law QP n=1e6 m=5e5, stoptol 1e-8, {large_iters} iterations",
+                           instances.config1(), 1e-8, large_iters)
+    return out
+
+
+def spmv_leg(peak_gbs: float, reps: int = 10, scale: float = 1.0):
     """Row-tiled SpMV on the large power-law QP's A and Q (device timing),
     beside the gather bound of the same matrix (hprqp_b200_gather_bound)."""
     import hprqp
     from hprqp import instances
 
-    inst = instances.config1()
+    inst = instances.config1(scale=scale)
     rng = np.random.default_rng(5)
     out = {}
     for name, (ip, ii, dd, nrow, ncol) in {
@@ -261,7 +352,7 @@ def spmv_leg(peak_gbs: float, reps: int = 10):
     return out
 
 
-def large_qp_leg(peak_gbs: float, iters: int = 3000, minres_iters: int = 2000):
+def large_qp_leg(peak_gbs: float, iters: int = 3000, minres_iters: int = 2000, scale: float = 1.0):
     """Plain solve_gpu on the large power-law QP (n=1e6, m=5e5, nnz(A)~1e7,
     nnz(Q)~3.2e7, stoptol 1e-8) for a fixed iteration budget (it does not
     reach 1e-8 within minutes, neither here nor with the reference's GPU
@@ -271,7 +362,7 @@ def large_qp_leg(peak_gbs: float, iters: int = 3000, minres_iters: int = 2000):
     import hprqp
     from hprqp import instances
 
-    inst = instances.config1()
+    inst = instances.config1(scale=scale)
     model = hprqp.build_from_instance(inst)
     params = hprqp.Parameters(verbose=False, stoptol=1e-8, max_iter=iters)
     t0 = time.perf_counter()
@@ -452,10 +543,18 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-plain-large", action="store_true")
     ap.add_argument("--no-warm", action="store_true")
-    ap.add_argument("--only", choices=["spmv", "batch", "adjoint", "large", "portfolio", "warm"], default=None,
+    ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--only", choices=["spmv", "batch", "adjoint", "large", "portfolio", "warm", "reference_gpu"],
+                    default=None,
                     help="sub-runs: only the large-QP SpMV leg, the batched solve, the adjoint, the large-QP "
-                         "plain solve, the portfolio plain solve or the warm-start re-solve")
+                         "plain solve, the portfolio plain solve, the warm-start re-solve or the reference GPU "
+                         "build beside the plain path")
     ap.add_argument("--spmv-reps", type=int, default=10)
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="--only spmv / --only large: the large power-law QP recipe with every dimension scaled "
+                         "(small cases for kernel profiles)")
+    ap.add_argument("--large-iters", type=int, default=3000, help="--only large: HPR iteration budget")
+    ap.add_argument("--minres-iters", type=int, default=2000, help="--only large: MINRES iteration budget")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -485,6 +584,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators)",
                 "config": config, "impl": "reference",
                 "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": kind,
+                                 "cpu_model": cpu_model(),
                                  "sample": f"{sample} batch instances per step, one process per core"},
                 "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -503,16 +603,20 @@ def main():
 
     peak, peak_kind = _peaks()
     if args.only == "spmv":
-        print(json.dumps({"spmv": spmv_leg(peak, args.spmv_reps)}), flush=True)
+        print(json.dumps({"spmv": spmv_leg(peak, args.spmv_reps, args.scale)}), flush=True)
         return
     if args.only == "adjoint":
         print(json.dumps({"adjoint": adjoint_leg(local_rank)}), flush=True)
         return
     if args.only == "large":
-        print(json.dumps({"large_qp": large_qp_leg(peak)}), flush=True)
+        print(json.dumps({"large_qp": large_qp_leg(peak, args.large_iters, args.minres_iters, args.scale)}),
+              flush=True)
         return
     if args.only == "portfolio":
         print(json.dumps({"portfolio": portfolio_leg()}), flush=True)
+        return
+    if args.only == "reference_gpu":
+        print(json.dumps({"reference_gpu": reference_gpu_leg(local_rank)}), flush=True)
         return
     insts = batch_instances(args.batch, rank_first_instance(rank))
     packed = hb.pack(insts)
@@ -602,11 +706,17 @@ def main():
         if not args.no_plain_large:
             line["large_qp"] = large_qp_leg(peak)
             line["portfolio"] = portfolio_leg()
+        if not args.no_reference_gpu:
+            line["reference_gpu"] = reference_gpu_leg(local_rank)
         ids = list(range(min(args.cpu_sample, args.batch)))
-        rate, kind, cdt, _ = cpu_reference_rate(ids, cores)
+        rate, kind, cdt, ref_solved = cpu_reference_rate(ids, cores)
         line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind,
+                                "cpu_model": cpu_model(),
                                 "sample": f"{len(ids)} batch instances, one process per core",
                                 "single_core": cpu_single_core_timings()}
+        # parity of the timed batch itself: its objectives against the
+        # reference CPU solves of the same instances
+        line["vs_reference_cpu"] = objective_agreement(res.status, res.objective, ref_solved)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -11,10 +11,17 @@
 // sigma are therefore per instance, and an instance that converges frees
 // its CTA for the next one immediately.
 //
-// Inside a CTA, y = M x runs over 32-row warp tiles whose lane-group width
-// is chosen per tile from the instance's own row lengths (the per-instance
-// SpMV autotuner); every reduction is folded in a fixed order, so each
-// instance's result is independent of which CTA solved it.
+// Inside a CTA, y = M x gives every warp a contiguous range of rows and
+// runs it as a CSR-vector product: a group of g lanes shares a row (32/g
+// rows per pass), each lane issues kU independent index/value loads per
+// round, and the group folds its partial sums with g-1 shuffles.  The group
+// width g of each matrix (Q, A, A') of each instance is chosen on the host
+// when the batch is packed, from that matrix's sequence of row lengths, by a
+// cost model of the rounds, passes and shuffles every warp would run (the
+// per-instance SpMV autotuner, choose_lane_group).  The choice is structural,
+// so an instance sums in the same order in every solve; every reduction is
+// folded in a fixed order, so each instance's result is independent of which
+// CTA solved it.
 #include "engine.h"
 #include "hprqp_batch.h"
 #include "hprqp.h"
@@ -47,13 +54,15 @@ namespace hpr {
 #ifndef HPR_BATCH_VEC_SMEM
 #define HPR_BATCH_VEC_SMEM 1
 #endif
+#ifndef HPR_BATCH_U
+#define HPR_BATCH_U 4
+#endif
 constexpr int kBT = HPR_BATCH_THREADS;  // threads per CTA of the batch kernel
 constexpr int kBW = kBT / 32;
-constexpr int kWin = 256;  // entries per warp window of the flat SpMV (8 per lane)
-constexpr size_t kScratchBytes = (size_t)kBW * kWin * sizeof(double);
+constexpr int kU = HPR_BATCH_U;  // independent index/value loads per lane per round of the SpMV
 // dynamic shared memory per CTA: half an SM, so that two CTAs fit; the
-// gathered vectors move to shared memory only when they fit beside the
-// scratch (small instances), else they stay in global memory (L1-cached)
+// gathered vectors move to shared memory when they fit (every instance of
+// n, m <= 2000), else they stay in global memory (L1-cached)
 constexpr size_t kSmemLimit = 110 * 1024;
 
 struct BInst {
@@ -61,6 +70,7 @@ struct BInst {
     int q_rp, a_rp, at_rp;        // first row pointer
     int var, row;                 // first variable / row in the packed vectors
     int n, m;
+    int q_lg, a_lg, at_lg;        // log2 of the SpMV lane-group width of Q, A, A' (0..5)
     double obj_constant;
 };
 
@@ -84,6 +94,10 @@ struct BatchArgs {
     int print_frequency;
     int use_scaling;
     unsigned long long t_start;  // globaltimer at launch (ns), set by CTA 0
+    // host-mapped flag set by hprqp_batch_request_abort (nonzero: stop);
+    // read by thread 0 of each CTA when an instance starts and every
+    // kAbortPoll iterations
+    const int *abort_flag;
     // outputs (packed like the inputs)
     double *x, *y, *z, *w;
     int *status;
@@ -100,6 +114,17 @@ struct BatchArgs {
     const double *sigma_start;  // per instance, optional (<= 0: from the data)
     double *sigma_out;          // per instance: sigma at the end of the solve
     double *seconds_out;        // per instance: device time from its start to its end on its CTA
+    // single-QP solves (solve_gpu of a small model runs as a batch of one):
+    // the time limit counts from the start of the instance's iteration loop,
+    // as the host loop's does (after setup); optional milestone, loop-time
+    // and log outputs
+    int time_from_loop;
+    long long *iter4_out, *iter6_out;  // first checked iteration with KKT < 1e-4 / 1e-6 (-1: none)
+    double *time4_out, *time6_out;     // loop seconds at those iterations
+    double *loop_seconds_out;          // loop seconds at the end
+    double *log_buf;                   // kLogFields doubles per printed iteration (instance 0 only)
+    int log_cap;
+    int *log_count;
 };
 
 // optional per-CTA phase clocks: 0 load+scale, 1 setup norms/diag, 2 power
@@ -119,12 +144,26 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     return t;
 }
 
+constexpr int kAbortPoll = 16;  // iterations between reads of the host abort flag
+// one log record: iter, errRp, errRd, primal obj, dual obj, gap, sigma, loop seconds
+constexpr int kLogFields = 8;
+
+// the host's abort request (a system-scope read of host-mapped memory)
+__device__ __forceinline__ bool abort_requested(const int *flag)
+{
+    if (!flag) return false;
+    int v;
+    asm volatile("ld.relaxed.sys.global.s32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+    return v != 0;
+}
+
 // local CSR view of one instance's matrix
 struct LCsr {
     int nrow;
     const int *rp;
     const int *ci;
     const double *v;
+    int lg;  // log2 of the lanes that share a row in cta_spmv
 };
 
 __device__ __forceinline__ double clampd(double v, double lo, double hi)
@@ -155,48 +194,66 @@ __device__ __forceinline__ void cta_allreduce(double (&v)[N], const int (&ops)[N
     for (int k = 0; k < N; ++k) v[k] = s_out[k];
 }
 
-// y = M x over 32-row warp tiles; f(row, y_row) is called by the lane that
-// owns the row (coalesced over consecutive rows).  A warp reads its tile's
-// entries as one flat, coalesced stream: eight independent index/value loads
-// per lane per 256-entry window, products staged in the warp's scratch, then
-// lane i adds row i's products in order.
+// Rows of a matrix with nrow rows that warp `warp` owns in cta_spmv: one
+// contiguous range per warp.  It depends on nrow only, so products with Q
+// and A' (both n rows) call their epilogues for a row on the same thread.
+__device__ __forceinline__ void warp_rows(int nrow, int warp, int &r0, int &r1)
+{
+    const int per = (nrow + kBW - 1) / kBW;
+    r0 = min(warp * per, nrow);
+    r1 = min(r0 + per, nrow);
+}
+
+// y = M x; f(row, y_row) is called by the lane that owns the row, on 32
+// consecutive rows per warp at a time (coalesced epilogues).
+//
+// Each warp walks its rows in chunks of 32: the chunk's row pointers are
+// read once (one per lane), then passes of 32/g rows run with g lanes per
+// row.  In a round every lane of a group loads kU entries of its row (lane
+// j of the group takes entries j, j+g, ..., all loads issued before the
+// gathers), multiplies them into its own sum in entry order; the group then
+// folds its g sums with an xor-shuffle tree and the row's value moves to
+// the lane that owns the row.  The summation order depends on g only.
 template <class F>
-__device__ __forceinline__ void cta_spmv(const LCsr &M, const double *x, double *scratch, F &&f)
+__device__ __forceinline__ void cta_spmv(const LCsr &M, const double *x, F &&f)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double *sc = scratch + warp * kWin;
-    const int ntiles = (M.nrow + 31) >> 5;
-    for (int t = warp; t < ntiles; t += kBW) {
-        const int r0 = t << 5;
-        const int nr = min(32, M.nrow - r0);
-        const int k0 = M.rp[r0], k1 = M.rp[r0 + nr];
-        const int a = lane < nr ? M.rp[r0 + lane] : k1;
-        const int e = lane < nr ? M.rp[r0 + lane + 1] : k1;
+    const int lg = M.lg, g = 1 << lg, sh = 5 - lg, rpp = 32 >> lg;
+    const int gl = lane & (g - 1), grp = lane >> lg;
+    int w0, w1;
+    warp_rows(M.nrow, warp, w0, w1);
+    for (int c0 = w0; c0 < w1; c0 += 32) {
+        const int nr = min(32, w1 - c0);
+        const int my_b = lane < nr ? M.rp[c0 + lane] : 0;
+        const int my_e = lane < nr ? M.rp[c0 + lane + 1] : 0;
         double mine = 0.0;
-        for (int base = k0; base < k1; base += kWin) {
-            int c[8];
-            double v[8];
+        const int passes = (nr + rpp - 1) >> sh;
+        for (int p = 0; p < passes; ++p) {
+            const int rr = (p << sh) + grp;  // row of the chunk this group sums (< 32)
+            const int b = __shfl_sync(0xffffffffu, my_b, rr);
+            const int e = __shfl_sync(0xffffffffu, my_e, rr);
+            double s = 0.0;
+            if (rr < nr) {
+                for (int k = b + gl; k < e; k += g * kU) {
+                    int c[kU];
+                    double v[kU];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int k = base + u * 32 + lane;
-                c[u] = k < k1 ? HPR_BATCH_LD(M.ci + k) : 0;
-                v[u] = k < k1 ? HPR_BATCH_LD(M.v + k) : 0.0;
-            }
+                    for (int u = 0; u < kU; ++u) {
+                        const int kk = k + u * g;
+                        c[u] = kk < e ? HPR_BATCH_LD(M.ci + kk) : 0;
+                        v[u] = kk < e ? HPR_BATCH_LD(M.v + kk) : 0.0;
+                    }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) sc[u * 32 + lane] = v[u] * x[c[u]];
-            __syncwarp();
-            const int lo = max(a, base), hi = min(e, base + kWin);
-            double s0 = 0.0, s1 = 0.0;
-            int j = lo;
-            for (; j + 1 < hi; j += 2) {
-                s0 += sc[j - base];
-                s1 += sc[j + 1 - base];
+                    for (int u = 0; u < kU; ++u)
+                        if (k + u * g < e) s = fma(v[u], x[c[u]], s);
+                }
             }
-            if (j < hi) s0 += sc[j - base];
-            mine += s0 + s1;
-            __syncwarp();
+            for (int o = g >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            // rows p*rpp .. p*rpp+rpp-1 of the chunk sit on lanes 0, g, 2g, ...
+            const double val = __shfl_sync(0xffffffffu, s, (lane & (rpp - 1)) << lg);
+            if ((lane >> sh) == p) mine = val;
         }
-        if (lane < nr) f(r0 + lane, mine);
+        if (lane < nr) f(c0 + lane, mine);
     }
 }
 
@@ -213,6 +270,8 @@ struct CtaState {
     double rp, rd, kkt, pobj, dobj, gap;
     double norm_b_org, norm_c_org, obj_constant;
     int to_check, do_res, stop, final_status;
+    int aborted;  // the host asked the batch to stop (sticky for the instance)
+    int print_yes, got4, got6;
     double red[16];
     double scal[8];
 };
@@ -278,7 +337,7 @@ __device__ __forceinline__ double row_abs(const LCsr &M, int r, bool sum)
 
 // Power iteration (reference src/gpu/eigs.cu:185-383), CTA-wide.
 static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q, bool is_a, int len, double *z, double *q,
-                            double *tmp, double *scratch, double (*s_red)[8], double *s_out)
+                            double *tmp, double (*s_red)[8], double *s_out)
 {
     if (len == 0) return 0.0;
     const int tid = threadIdx.x;
@@ -301,15 +360,15 @@ static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q,
         double v2[2] = {0.0, 0.0};
         const int ops2[2] = {kSum, kSum};
         if (is_a) {
-            cta_spmv(AT, q, scratch, [&](int r, double s) { tmp[r] = s; });
+            cta_spmv(AT, q, [&](int r, double s) { tmp[r] = s; });
             __syncthreads();
-            cta_spmv(A, tmp, scratch, [&](int r, double s) {
+            cta_spmv(A, tmp, [&](int r, double s) {
                 z[r] = s;
                 v2[0] += q[r] * s;
                 v2[1] += s * s;
             });
         } else {
-            cta_spmv(Q, q, scratch, [&](int r, double s) {
+            cta_spmv(Q, q, [&](int r, double s) {
                 z[r] = s;
                 v2[0] += q[r] * s;
                 v2[1] += s * s;
@@ -344,30 +403,59 @@ static __device__ __forceinline__ size_t adaptive_step_d(long long iter)
 __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs B)
 {
     extern __shared__ __align__(16) double dyn_smem[];
-    double *scratch = dyn_smem;  // kBW * kWin
     __shared__ CtaState S;
     __shared__ double s_red[kBW][8];
     __shared__ double s_out[8];
-    __shared__ int s_inst;
+    __shared__ int s_inst, s_skip;
     const int tid = threadIdx.x;
     Vecs V = carve(B.ws + (size_t)blockIdx.x * B.ws_stride, B.nmax, B.mmax,
-                   B.vec_smem ? dyn_smem + kBW * kWin : nullptr);
+                   B.vec_smem ? dyn_smem : nullptr);
 
     for (;;) {
         if (tid == 0) {
             const int slot = atomicAdd(B.counter, 1);
             s_inst = slot < B.K ? B.order[slot] : -1;
+            // an instance taken after the batch's time limit or after an
+            // abort request is not set up: it reports TIME_LIMIT at iteration
+            // 0 with zero vectors and infinite residuals
+            s_skip = s_inst >= 0 && (abort_requested(B.abort_flag) ||
+                                     1e-9 * (double)(globaltimer_ns() - B.t_start) > B.time_limit);
         }
         __syncthreads();
         const int k = s_inst;
+        const bool skip = s_skip;
         __syncthreads();
         if (k < 0) break;
-        const unsigned long long inst_t0 = globaltimer_ns();
         const BInst I = B.inst[k];
         const int n = I.n, m = I.m;
-        LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz};
-        LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz};
-        LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz};
+        if (skip) {
+            for (int i = tid; i < n; i += kBT) {
+                B.x[I.var + i] = B.w[I.var + i] = B.z[I.var + i] = 0.0;
+                if (B.active_x) B.active_x[I.var + i] = 0;
+                B.col_norm_out[I.var + i] = 1.0;
+            }
+            for (int i = tid; i < m; i += kBT) {
+                B.y[I.row + i] = 0.0;
+                if (B.active_r) B.active_r[I.row + i] = 0;
+                B.row_norm_out[I.row + i] = 1.0;
+            }
+            if (tid == 0) {
+                B.status[k] = 5;
+                B.iters[k] = 0;
+                B.pobj[k] = 0.0;
+                B.resid[k] = INFINITY;
+                B.gap[k] = INFINITY;
+                B.restarts[k] = 0;
+                B.sigma_out[k] = 0.0;
+                B.seconds_out[k] = 0.0;
+            }
+            __syncthreads();
+            continue;
+        }
+        const unsigned long long inst_t0 = globaltimer_ns();
+        LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz, I.q_lg};
+        LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz, I.a_lg};
+        LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz, I.at_lg};
         double *qv = B.q_v + I.q_nz, *av = B.a_v + I.a_nz, *atv = B.at_v + I.at_nz;
         const int q_nnz = Q.rp[n], a_nnz = m > 0 ? A.rp[m] : 0;
 
@@ -492,11 +580,11 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
         }
         PHASE_ADD(1);
         if (!S.q_is_diag) {
-            const double lq = (q_nnz > 0) ? cta_power(A, AT, Q, false, n, V.pn, V.tempv, V.Qx, scratch, s_red, s_out) : 0.0;
+            const double lq = (q_nnz > 0) ? cta_power(A, AT, Q, false, n, V.pn, V.tempv, V.Qx, s_red, s_out) : 0.0;
             if (tid == 0) S.lQ = lq * 1.05;
         }
         {
-            const double la = m > 0 ? cta_power(A, AT, Q, true, m, V.pz, V.pq, V.pn, scratch, s_red, s_out) : 0.0;
+            const double la = m > 0 ? cta_power(A, AT, Q, true, m, V.pz, V.pq, V.pn, s_red, s_out) : 0.0;
             if (tid == 0) S.lA = la * 1.05;
         }
         __syncthreads();
@@ -531,8 +619,8 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             // the products the step carries with the iterates: A'y, and Q w
             // on the noC path (reference iteration.cu:831-920)
             if (m > 0)
-                cta_spmv(AT, V.y, scratch, [&](int i, double s) { V.ATy[i] = V.ATy_bar[i] = V.last_ATy[i] = s; });
-            if (S.noC) cta_spmv(Q, V.w, scratch, [&](int i, double s) { V.Qw[i] = V.Qw_bar[i] = V.last_Qw[i] = s; });
+                cta_spmv(AT, V.y, [&](int i, double s) { V.ATy[i] = V.ATy_bar[i] = V.last_ATy[i] = s; });
+            if (S.noC) cta_spmv(Q, V.w, [&](int i, double s) { V.Qw[i] = V.Qw_bar[i] = V.last_Qw[i] = s; });
         }
         if (tid == 0) {
             S.restart_flag = 0;
@@ -542,18 +630,19 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             S.best_sigma = S.sigma;
             S.inner = 0;
             S.times = 0;
+            S.aborted = 0;
         }
         __syncthreads();
 
         // ---- residuals (reference residuals.cu:81-183) ----------------------
         auto residuals = [&](long long iter) {
-            if (m > 0) cta_spmv(AT, V.y_bar, scratch, [&](int r, double s) { V.ATdy[r] = s; });
+            if (m > 0) cta_spmv(AT, V.y_bar, [&](int r, double s) { V.ATdy[r] = s; });
             else
                 for (int i = tid; i < n; i += kBT) V.ATdy[i] = 0.0;
             double a[3] = {0.0, 0.0, 0.0};
             const int opa[3] = {kMax, kMax, kSum};
             if (m > 0)
-                cta_spmv(A, V.x_bar, scratch, [&](int r, double ax) {
+                cta_spmv(A, V.x_bar, [&](int r, double ax) {
                     const double proj = clampd(ax, V.AL[r], V.AU[r]);
                     const double sf = V.row_norm[r];
                     V.Ax[r] = ax;
@@ -565,7 +654,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             __syncthreads();
             double q[7] = {0, 0, 0, 0, 0, 0, 0};
             const int opq[7] = {kMax, kMax, kMax, kSum, kSum, kSum, kMax};
-            cta_spmv(Q, V.x_bar, scratch, [&](int r, double qx) {
+            cta_spmv(Q, V.x_bar, [&](int r, double qx) {
                 const double sf = V.col_norm[r];
                 const double xb = V.x_bar[r], aty = V.ATdy[r];
                 V.Qx[r] = qx;
@@ -623,11 +712,11 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
                     V.w_bar[i] = wb;
                     V.w[i] = h2 * (2.0 * wb - wi) + h1 * V.last_w[i];
                 };
-                if (m > 0) cta_spmv(AT, V.y, scratch, upd);
+                if (m > 0) cta_spmv(AT, V.y, upd);
                 else
                     for (int i = tid; i < n; i += kBT) upd(i, 0.0);
                 __syncthreads();
-                cta_spmv(Q, V.w_bar, scratch, [&](int i, double qwb) {
+                cta_spmv(Q, V.w_bar, [&](int i, double qwb) {
                     const double qw = V.Qw[i];
                     V.Qw_bar[i] = qwb;
                     V.Qw[i] = h2 * (2.0 * qwb - qw) + h1 * V.last_Qw[i];
@@ -635,7 +724,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
                 });
                 __syncthreads();
             } else {
-                cta_spmv(Q, V.w, scratch, [&](int i, double qw) {
+                cta_spmv(Q, V.w, [&](int i, double qw) {
                     const double xi = V.x[i], wi = V.w[i];
                     const double z_raw = xi + sigma * (-qw + V.ATy[i] - V.c[i]);
                     const double xb = clampd(z_raw, V.l[i], V.u[i]);
@@ -652,14 +741,14 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
                 });
                 __syncthreads();
                 if (m > 0) {
-                    cta_spmv(Q, V.w_bar, scratch,
+                    cta_spmv(Q, V.w_bar,
                              [&](int i, double qwb) { V.tempv[i] = V.x_hat[i] + sigma * (V.Qw[i] - qwb); });
                     __syncthreads();
                 }
             }
             if (m > 0) {
                 const double f1 = lA * sigma, f2 = 1.0 / f1;
-                cta_spmv(A, V.tempv, scratch, [&](int i, double ax) {
+                cta_spmv(A, V.tempv, [&](int i, double ax) {
                     const double yi = V.y[i];
                     const double s_raw = ax - f1 * yi;
                     const double sp = clampd(s_raw, V.AL[i], V.AU[i]);
@@ -689,7 +778,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
                     V.w[i] = h1 * V.last_w[i] + h2 * (2.0 * wbn - wi);
                     V.ATy[i] = h1 * V.last_ATy[i] + h2 * (2.0 * atyb - aty);
                 };
-                if (m > 0) cta_spmv(AT, V.y_bar, scratch, w2);
+                if (m > 0) cta_spmv(AT, V.y_bar, w2);
                 else
                     for (int i = tid; i < n; i += kBT) w2(i, 0.0);
                 __syncthreads();
@@ -700,7 +789,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
         auto m_norm = [&]() -> double {
             double a[4] = {0, 0, 0, 0};
             const int ops4[4] = {kSum, kSum, kSum, kSum};
-            cta_spmv(Q, V.dw, scratch, [&](int i, double v) {
+            cta_spmv(Q, V.dw, [&](int i, double v) {
                 V.dQw[i] = v;
                 const double dx = V.dx[i];
                 a[0] += dx * dx;
@@ -712,13 +801,13 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             double b[2] = {0, 0}, c3[3] = {0, 0, 0};
             const int ops2[2] = {kSum, kSum}, ops3[3] = {kSum, kSum, kSum};
             if (m > 0) {
-                cta_spmv(AT, V.dy, scratch, [&](int i, double v) {
+                cta_spmv(AT, V.dy, [&](int i, double v) {
                     V.ATdy[i] = v;
                     b[0] += v * V.dx[i];
                 });
                 for (int i = tid; i < m; i += kBT) b[1] += V.dy[i] * V.dy[i];
                 __syncthreads();
-                cta_spmv(Q, V.ATdy, scratch, [&](int i, double v) {
+                cta_spmv(Q, V.ATdy, [&](int i, double v) {
                     V.QATdy[i] = v;
                     const double at = V.ATdy[i];
                     c3[0] += V.dQw[i] * at;
@@ -770,14 +859,14 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             __syncthreads();
             double e3[3] = {0, 0, 0}, f1v[1] = {0};
             const int ops3[3] = {kSum, kSum, kSum}, ops1[1] = {kSum};
-            cta_spmv(Q, V.dw, scratch, [&](int i, double v) {
+            cta_spmv(Q, V.dw, [&](int i, double v) {
                 V.dQw[i] = v;
                 if (m > 0) e3[0] += v * V.ATdy[i];
                 e3[1] += v * v;
                 e3[2] += V.dw[i] * v;
             });
             if (m > 0) {
-                cta_spmv(Q, V.ATdy, scratch, [&](int i, double v) {
+                cta_spmv(Q, V.ATdy, [&](int i, double v) {
                     V.QATdy[i] = v;
                     f1v[0] += V.ATdy[i] * v;
                 });
@@ -893,7 +982,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             }
             for (int i = tid; i < m; i += kBT) V.y[i] = V.last_y[i] = V.y_bar[i];
             if (m > 0) {
-                cta_spmv(AT, V.y_bar, scratch, [&](int i, double s) { V.ATy_bar[i] = V.ATy[i] = V.last_ATy[i] = s; });
+                cta_spmv(AT, V.y_bar, [&](int i, double s) { V.ATy_bar[i] = V.ATy[i] = V.last_ATy[i] = s; });
             }
             __syncthreads();
             if (tid == 0) {
@@ -906,22 +995,65 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
         };
 
         // ---- outer loop (reference solver_backend.c:432-513) ------------------
+        const unsigned long long loop_t0 = globaltimer_ns();  // used by thread 0
+        // one log record of the current residuals (the host loop's print_log)
+        auto log_record = [&](long long it) {
+            if (!B.log_buf || k != 0) return;
+            const int slot = *B.log_count;
+            if (slot >= B.log_cap) return;
+            double *r = B.log_buf + (size_t)slot * kLogFields;
+            r[0] = (double)it;
+            r[1] = S.rp;
+            r[2] = S.rd;
+            r[3] = S.pobj;
+            r[4] = S.dobj;
+            r[5] = S.gap;
+            r[6] = S.sigma;
+            r[7] = 1e-9 * (double)(globaltimer_ns() - loop_t0);
+            *B.log_count = slot + 1;
+        };
+        // first checked iteration below 1e-4 / 1e-6 (the host loop's milestones)
+        auto milestones = [&](long long it) {
+            const double el = 1e-9 * (double)(globaltimer_ns() - loop_t0);
+            if (!S.got4 && S.kkt < 1e-4) {
+                S.got4 = 1;
+                if (B.iter4_out) {
+                    B.iter4_out[k] = it;
+                    B.time4_out[k] = el;
+                }
+            }
+            if (!S.got6 && S.kkt < 1e-6) {
+                S.got6 = 1;
+                if (B.iter6_out) {
+                    B.iter6_out[k] = it;
+                    B.time6_out[k] = el;
+                }
+            }
+        };
         residuals(0);
+        if (tid == 0) {
+            S.got4 = S.got6 = 0;
+            if (B.iter4_out) B.iter4_out[k] = B.iter6_out[k] = -1;
+            milestones(0);
+            log_record(0);
+        }
         long long iter;
         for (iter = 0;; ++iter) {
             if (tid == 0) {
-                const double el = 1e-9 * (double)(globaltimer_ns() - B.t_start);
+                const double el = 1e-9 * (double)(globaltimer_ns() - (B.time_from_loop ? loop_t0 : B.t_start));
+                if (iter % kAbortPoll == 0 && !S.aborted && abort_requested(B.abort_flag)) S.aborted = 1;
+                // an abort request stops the instance like the time limit
+                const bool over = el > B.time_limit || S.aborted;
                 int print_yes = 0;
                 if (iter > 0) {
                     if (B.print_frequency == -1 &&
-                        ((long long)(iter % (long long)adaptive_step_d(iter)) == 0 || iter == B.max_iter ||
-                         el > B.time_limit))
+                        ((long long)(iter % (long long)adaptive_step_d(iter)) == 0 || iter == B.max_iter || over))
                         print_yes = 1;
-                    if (B.print_frequency > 0 &&
-                        (iter % B.print_frequency == 0 || iter == B.max_iter || el > B.time_limit))
+                    if (B.print_frequency > 0 && (iter % B.print_frequency == 0 || iter == B.max_iter || over))
                         print_yes = 1;
                 }
                 S.do_res = iter > 0 && ((B.check_iter > 0 && iter % B.check_iter == 0) || print_yes);
+                S.print_yes = print_yes;
                 S.scal[1] = el;
             }
             __syncthreads();
@@ -930,13 +1062,14 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             PHASE_ADD(4);
             if (tid == 0) {
                 const double el = S.scal[1];
+                if (S.do_res) milestones(iter);
                 int fs;
                 // a warm start is not an HPR iterate: its y and z need not lie
                 // in the normal cones the residual formulas assume, so it is
                 // not accepted as optimal before the first step
                 if (S.kkt < B.stoptol && !(warm && iter == 0)) fs = 6;
                 else if (iter == B.max_iter) fs = 4;
-                else if (el > B.time_limit) fs = 5;
+                else if (el > B.time_limit || S.aborted) fs = 5;
                 else fs = 7;
                 S.final_status = fs;
                 // restart_check (src/cpu/control.c:231-282)
@@ -972,6 +1105,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
                 restart_apply();
             }
             PHASE_ADD(6);
+            if (tid == 0 && (S.print_yes || S.final_status != 7)) log_record(iter);
             if (S.final_status != 7) break;
             if (tid == 0) {
                 const long long nx = iter + 1;
@@ -1025,6 +1159,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             B.restarts[k] = (int)S.times;
             B.sigma_out[k] = S.sigma;
             B.seconds_out[k] = 1e-9 * (double)(globaltimer_ns() - inst_t0);
+            if (B.loop_seconds_out) B.loop_seconds_out[k] = 1e-9 * (double)(globaltimer_ns() - loop_t0);
         }
         __syncthreads();
     }
@@ -1070,15 +1205,13 @@ constexpr int kAdjLanczos = 3;                   // v_old, v, v_new (n and m par
 __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_adjoint(const AdjArgs B)
 {
     extern __shared__ __align__(16) double dyn_smem[];
-    double *scratch = dyn_smem;
     __shared__ double s_red[kBW][8];
     __shared__ double s_out[8];
     __shared__ int s_inst;
     const int tid = threadIdx.x;
     const int na = (B.nmax + 31) & ~31, ma = (B.mmax + 31) & ~31;
     double *g = B.ws + (size_t)blockIdx.x * B.ws_stride;
-    double *lz = B.lanczos_smem ? dyn_smem + kBW * kWin
-                                : g + kAdjGlobalN * (size_t)na + kAdjGlobalM * (size_t)ma;
+    double *lz = B.lanczos_smem ? dyn_smem : g + kAdjGlobalN * (size_t)na + kAdjGlobalM * (size_t)ma;
     for (;;) {
         if (tid == 0) {
             const int slot = atomicAdd(B.counter, 1);
@@ -1090,9 +1223,9 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_adjoint(const AdjArgs
         if (k < 0) break;
         const BInst I = B.inst[k];
         const int n = I.n, m = I.m;
-        const LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz};
-        const LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz};
-        const LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz};
+        const LCsr Q{n, B.q_rp + I.q_rp, B.q_ci + I.q_nz, B.q_v + I.q_nz, I.q_lg};
+        const LCsr A{m, B.a_rp + I.a_rp, B.a_ci + I.a_nz, B.a_v + I.a_nz, I.a_lg};
+        const LCsr AT{n, B.at_rp + I.at_rp, B.at_ci + I.at_nz, B.at_v + I.at_nz, I.at_lg};
         const double *cn = B.col_norm + I.var, *rn = B.row_norm + I.row;
         const double *zk = B.z + I.var, *yk = B.y + I.row;
         double *sol_n = g, *wo_n = g + na, *w_n = g + 2 * na, *wn_n = g + 3 * na, *tmp = g + 4 * na;
@@ -1126,15 +1259,16 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_adjoint(const AdjArgs
             __syncthreads();
             const int maxit = B.maxit_factor * (n + m) + 100;
             for (it = 0; it < maxit; ++it) {
-                // v_new = P Ks P v.  Q and A' have the same 32-row tiling, so
-                // tmp[i] is written and read by the same thread.
+                // v_new = P Ks P v.  Q and A' have the same number of rows, so
+                // cta_spmv calls their epilogues for row i on the same thread
+                // and tmp[i] is written and read by that thread.
                 if (m > 0) {
-                    cta_spmv(Q, v_n, scratch, [&](int i, double q) { tmp[i] = q; });
-                    cta_spmv(A, v_n, scratch, [&](int r, double a) { vn_m[r] = yk[r] != 0.0 ? a : 0.0; });
-                    cta_spmv(AT, v_m, scratch,
+                    cta_spmv(Q, v_n, [&](int i, double q) { tmp[i] = q; });
+                    cta_spmv(A, v_n, [&](int r, double a) { vn_m[r] = yk[r] != 0.0 ? a : 0.0; });
+                    cta_spmv(AT, v_m,
                              [&](int i, double at) { vn_n[i] = zk[i] == 0.0 ? tmp[i] + at : 0.0; });
                 } else {
-                    cta_spmv(Q, v_n, scratch, [&](int i, double q) { vn_n[i] = zk[i] == 0.0 ? q : 0.0; });
+                    cta_spmv(Q, v_n, [&](int i, double q) { vn_n[i] = zk[i] == 0.0 ? q : 0.0; });
                 }
                 __syncthreads();
                 double al[1] = {0.0};
@@ -1271,6 +1405,9 @@ struct HPRQPBatch {
     std::vector<int> n_k, m_k;                      // preprocessed sizes
     std::vector<std::vector<size_t>> kept_rows;     // per instance: original local row of each kept row
     std::vector<hpr::BInst> inst;
+    std::vector<int> tuned_lg;  // autotuned lane-group widths (log2), Q, A, A' per instance
+    int forced_lanes = 0;       // hprqp_batch_set_spmv_lanes: 0 = autotuned
+    hpr::BInst *d_inst = nullptr;
     size_t total_n = 0, total_m = 0, total_m_orig = 0;
     int nmax = 0, mmax = 0;
     std::vector<void *> allocs;
@@ -1290,6 +1427,8 @@ struct HPRQPBatch {
     // hprqp_batch_set_warm_start
     double *start_x = nullptr, *start_w = nullptr, *start_y = nullptr, *start_sigma = nullptr;
     unsigned long long *d_t0 = nullptr, *d_phase = nullptr;
+    // abort request: one int in host-mapped pinned memory, read by the kernel
+    int *h_abort = nullptr, *d_abort = nullptr;
     // host copies of the preprocessed models (kept for the adjoint)
     std::vector<HPRQPModel> models;
 };
@@ -1315,10 +1454,66 @@ static void batch_free(HPRQPBatch *b)
 {
     for (void *p : b->allocs) cudaFree(p);
     b->allocs.clear();
+    if (b->h_abort) cudaFreeHost(b->h_abort);
+    b->h_abort = b->d_abort = nullptr;
     for (auto &m : b->models) model_free(&m);
     b->models.clear();
     if (b->stream) cudaStreamDestroy(b->stream);
     b->stream = nullptr;
+}
+
+// The per-instance SpMV autotuner: the lane-group width of cta_spmv for one
+// matrix, from its row lengths.  For every width g = 1, 2, ..., 32 it walks
+// the rows exactly as cta_spmv does (kBW contiguous warp ranges, chunks of 32
+// rows, passes of 32/g rows, rounds of g*kU entries, the longest row of a
+// pass setting its rounds) and charges each warp
+//     kChunkCost per chunk + per pass (kPassCost + log2(g) kShuffleCost
+//     + rounds * kRoundCost);
+// the warp with the largest charge sets the product's time, and the width
+// with the smallest such time wins (ties: the wider group, whose loads are
+// better coalesced).  The charges are in units of about 50 SM cycles:
+// a round is a global load, a dependent gather and kU dependent FMAs, a
+// shuffle step is one shuffle of a double, a pass re-reads two row pointers
+// from registers and moves the row sums.  The weights come from timing
+// each forced width over the 4096-QP batch recipe (hprqp_batch_set_spmv_lanes).
+constexpr double kRoundCost = 12.0, kShuffleCost = 0.6, kPassCost = 1.5, kChunkCost = 4.0;
+
+static double lane_group_cost(const size_t *rp, int nrow, int lg)
+{
+    const int g = 1 << lg, rpp = 32 >> lg;
+    const int per = (nrow + kBW - 1) / kBW;
+    double worst = 0.0;
+    for (int w = 0; w < kBW; ++w) {
+        const int w0 = std::min(w * per, nrow), w1 = std::min(w0 + per, nrow);
+        double cost = 0.0;
+        for (int c0 = w0; c0 < w1; c0 += 32) {
+            const int nr = std::min(32, w1 - c0);
+            cost += kChunkCost;
+            for (int p0 = 0; p0 < nr; p0 += rpp) {
+                size_t longest = 0;
+                for (int r = c0 + p0; r < std::min(c0 + p0 + rpp, c0 + nr); ++r)
+                    longest = std::max(longest, rp[r + 1] - rp[r]);
+                const size_t rounds = (longest + (size_t)(g * kU) - 1) / (size_t)(g * kU);
+                cost += kPassCost + lg * kShuffleCost + (double)rounds * kRoundCost;
+            }
+        }
+        worst = std::max(worst, cost);
+    }
+    return worst;
+}
+
+static int choose_lane_group(const size_t *rp, int nrow)
+{
+    int best = 0;
+    double best_cost = 0.0;
+    for (int lg = 0; lg <= 5; ++lg) {
+        const double c = lane_group_cost(rp, nrow, lg);
+        if (lg == 0 || c <= best_cost) {
+            best = lg;
+            best_cost = c;
+        }
+    }
+    return best;
 }
 
 // extract instance k of a block-diagonal CSR (rows [r0, r1), columns
@@ -1404,7 +1599,7 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     b->has_caller_csr = keep_caller_csr;
     // ---- per-instance build + preprocess (the single-QP builder), threaded
     std::vector<HPRQPStatus> st_k(K, HPRQP_STATUS_OK);
-    const unsigned nth = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    const unsigned nth = (unsigned)std::max<size_t>(1, std::min<size_t>(std::min(std::thread::hardware_concurrency(), 32u), K));
     auto worker = [&](unsigned tix) {
         std::vector<size_t> qrp, qci, arp, aci;
         std::vector<double> qv, av;
@@ -1439,7 +1634,9 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     };
     {
         std::vector<std::thread> th;
-        for (unsigned t = 0; t < nth; ++t) th.emplace_back(worker, t);
+        if (nth == 1) worker(0);
+        else
+            for (unsigned t = 0; t < nth; ++t) th.emplace_back(worker, t);
         for (auto &t : th) t.join();
     }
     for (size_t k = 0; k < K; ++k)
@@ -1491,10 +1688,14 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         h_AL(std::max<size_t>(nr, 1)), h_AU(std::max<size_t>(nr, 1));
     h_qci[0] = h_aci[0] = h_atci[0] = 0;
     h_qv[0] = h_av[0] = h_atv[0] = h_c[0] = h_l[0] = h_u[0] = h_AL[0] = h_AU[0] = 0.0;
+    b->tuned_lg.assign(3 * K, 0);
     auto pack_worker = [&](unsigned tix) {
     for (size_t k = tix; k < K; k += nth) {
         const HPRQPModel &M = b->models[k];
-        const BInst &I = b->inst[k];
+        BInst &I = b->inst[k];
+        I.q_lg = b->tuned_lg[3 * k] = choose_lane_group(M.Q.row_ptr, (int)M.Q.nrow);
+        I.a_lg = b->tuned_lg[3 * k + 1] = choose_lane_group(M.A.row_ptr, (int)M.A.nrow);
+        I.at_lg = b->tuned_lg[3 * k + 2] = choose_lane_group(M.AT.row_ptr, (int)M.AT.nrow);
         for (size_t r = 0; r <= M.Q.nrow; ++r) h_qrp[I.q_rp + r] = (int)M.Q.row_ptr[r];
         for (size_t r = 0; r <= M.A.nrow; ++r) h_arp[I.a_rp + r] = (int)M.A.row_ptr[r];
         for (size_t r = 0; r <= M.AT.nrow; ++r) h_atrp[I.at_rp + r] = (int)M.AT.row_ptr[r];
@@ -1519,7 +1720,9 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     };
     {
         std::vector<std::thread> pth;
-        for (unsigned t = 0; t < nth; ++t) pth.emplace_back(pack_worker, t);
+        if (nth == 1) pack_worker(0);
+        else
+            for (unsigned t = 0; t < nth; ++t) pth.emplace_back(pack_worker, t);
         for (auto &t : pth) t.join();
     }
     const double c2 = cnow();
@@ -1578,7 +1781,13 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         !up(d_AU, h_AU.data(), h_AU.size() * 8) || !up(d_inst, b->inst.data(), K * sizeof(BInst)) ||
         !up(d_order, order.data(), K * sizeof(int)) || cudaStreamSynchronize(b->stream) != cudaSuccess)
         return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
+    if (cudaHostAlloc((void **)&b->h_abort, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&b->d_abort, b->h_abort, 0) != cudaSuccess)
+        return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
+    __atomic_store_n(b->h_abort, 0, __ATOMIC_SEQ_CST);
+    G.abort_flag = b->d_abort;
     G.inst = d_inst;
+    b->d_inst = d_inst;
     G.order = d_order;
     G.counter = d_counter;
     G.q_rp = d_qrp;
@@ -1621,8 +1830,8 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     BatchArgs &G = b->args;
     const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
     const size_t vec_bytes = (4 * na + 2 * ma) * sizeof(double);
-    G.vec_smem = HPR_BATCH_VEC_SMEM && kScratchBytes + vec_bytes <= kSmemLimit;
-    const size_t smem = kScratchBytes + (G.vec_smem ? vec_bytes : 0);
+    G.vec_smem = HPR_BATCH_VEC_SMEM && vec_bytes <= kSmemLimit;
+    const size_t smem = G.vec_smem ? vec_bytes : 0;
     B_CK(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve, kBT, smem));
@@ -1681,6 +1890,8 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     B_CK(cudaGetLastError());
     b->last_ms = ms;
     b->solved = true;
+    // an abort request ends with the solve it stopped
+    __atomic_store_n(b->h_abort, 0, __ATOMIC_SEQ_CST);
     if (d_phase) {
         std::vector<unsigned long long> h((size_t)grid * 8);
         B_CK(cudaMemcpy(h.data(), d_phase, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -1766,6 +1977,44 @@ double hprqp_batch_last_solve_ms(const HPRQPBatch *b) { return b ? b->last_ms : 
 
 size_t hprqp_batch_num_instances(const HPRQPBatch *b) { return b ? b->K : 0; }
 
+HPRQPStatus hprqp_batch_request_abort(HPRQPBatch *b)
+{
+    if (!b || !b->h_abort) return HPRQP_STATUS_INVALID_ARGUMENT;
+    __atomic_store_n(b->h_abort, 1, __ATOMIC_SEQ_CST);
+    return HPRQP_STATUS_OK;
+}
+
+HPRQPStatus hprqp_batch_set_spmv_lanes(HPRQPBatch *b, int lanes)
+{
+    using namespace hpr;
+    if (!b || !(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32))
+        return HPRQP_STATUS_INVALID_ARGUMENT;
+    int lg = 0;
+    while ((1 << lg) < lanes) ++lg;
+    for (size_t k = 0; k < b->K; ++k) {
+        BInst &I = b->inst[k];
+        I.q_lg = lanes ? lg : b->tuned_lg[3 * k];
+        I.a_lg = lanes ? lg : b->tuned_lg[3 * k + 1];
+        I.at_lg = lanes ? lg : b->tuned_lg[3 * k + 2];
+    }
+    B_CK(cudaSetDevice(b->device));
+    B_CK(cudaMemcpyAsync(b->d_inst, b->inst.data(), b->K * sizeof(BInst), cudaMemcpyHostToDevice, b->stream));
+    B_CK(cudaStreamSynchronize(b->stream));
+    b->forced_lanes = lanes;
+    return HPRQP_STATUS_OK;
+}
+
+HPRQPStatus hprqp_batch_get_spmv_lanes(const HPRQPBatch *b, int *lanes)
+{
+    if (!b || !lanes) return HPRQP_STATUS_INVALID_ARGUMENT;
+    for (size_t k = 0; k < b->K; ++k) {
+        lanes[3 * k] = 1 << b->inst[k].q_lg;
+        lanes[3 * k + 1] = 1 << b->inst[k].a_lg;
+        lanes[3 * k + 2] = 1 << b->inst[k].at_lg;
+    }
+    return HPRQP_STATUS_OK;
+}
+
 HPRQPStatus hprqp_batch_get_results(const HPRQPBatch *b, int *status, size_t *iter, double *primal_obj,
                                     double *residual, double *gap, double *x, double *y, double *z, double *w)
 {
@@ -1824,8 +2073,8 @@ HPRQPStatus hprqp_batch_backward(HPRQPBatch *b, const double *grad_x, const doub
     // ---- device buffers (first call only)
     const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
     const size_t lz_bytes = (size_t)kAdjLanczos * (na + ma) * sizeof(double);
-    const int lanczos_smem = kScratchBytes + lz_bytes <= kSmemLimit;
-    const size_t smem = kScratchBytes + (lanczos_smem ? lz_bytes : 0);
+    const int lanczos_smem = lz_bytes <= kSmemLimit;
+    const size_t smem = lanczos_smem ? lz_bytes : 0;
     B_CK(cudaFuncSetAttribute(k_batch_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_adjoint, kBT, smem));
@@ -2013,3 +2262,141 @@ HPRQPStatus hprqp_solve_batch(size_t K, const size_t *var_offsets, const size_t 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// small single QPs: solve_gpu as a batch of one
+// ---------------------------------------------------------------------------
+namespace hpr {
+
+// Models whose products per iteration stay below this many nonzeros
+// (2 nnz(Q) + 2 nnz(A)) run in one CTA of the batch kernel: a host-driven
+// iteration costs four kernel launches and the device-wide passes of the
+// plain engine, which small problems cannot fill.  Process-wide; set by
+// hprqp_b200_set_single_cta_max_work.
+static size_t g_single_cta_max_work = 200000;
+
+static size_t log_records_needed(const HPRQPParams *p)
+{
+    if (!p->verbose) return 0;
+    if (p->print_frequency > 0) return p->max_iter / (size_t)p->print_frequency + 4;
+    if (p->print_frequency == -1) return 2048;  // adaptive steps: < 100 per decade of iterations
+    return 4;
+}
+
+bool single_cta_eligible(const HPRQPModel *m, const HPRQPParams *p)
+{
+    if (!m || !p || m->num_var_cones || m->num_row_cones) return false;
+    if (m->Q.ncol == 0 || m->Q.ncol > (size_t)INT32_MAX || m->A.nrow > (size_t)INT32_MAX) return false;
+    if (2 * (m->Q.nnz + m->A.nnz) > g_single_cta_max_work) return false;
+    return log_records_needed(p) <= kSingleCtaLogCap;
+}
+
+HPRQPStatus solve_single_cta(const HPRQPModel *model, const HPRQPParams *params, HPRQPResults *results,
+                             double *log_records, size_t log_cap, size_t *log_count)
+{
+    if (log_count) *log_count = 0;
+    const size_t n = model->Q.ncol, m = model->A.nrow;
+    const size_t var_off[2] = {0, n}, row_off[2] = {0, m};
+    HPRQPBatch *b = nullptr;
+    // the model is already preprocessed; the builder's rules leave it unchanged
+    HPRQPStatus st = batch_create_impl(1, var_off, row_off, &model->Q, &model->A, model->c, model->AL, model->AU,
+                                       model->l, model->u, &model->obj_constant, params->device_number, false, &b);
+    if (st != HPRQP_STATUS_OK) return st;
+    BatchArgs &G = b->args;
+    long long *d_i4 = nullptr, *d_i6 = nullptr;
+    double *d_t = nullptr, *d_log = nullptr;
+    int *d_logn = nullptr;
+    const size_t cap = log_records ? std::min(log_cap, log_records_needed(params)) : 0;
+    if ((st = balloc(b, &d_i4, 1)) || (st = balloc(b, &d_i6, 1)) || (st = balloc(b, &d_t, 3)) ||
+        (st = balloc(b, &d_logn, 1)) || (cap && (st = balloc(b, &d_log, cap * kLogFields)))) {
+        hprqp_batch_destroy(b);
+        return st;
+    }
+    auto cuda_fail = [&](cudaError_t e, int line) {
+        fprintf(stderr, "hprqp-b200: CUDA error %s at %s:%d\n", cudaGetErrorString(e), __FILE__, line);
+        hprqp_batch_destroy(b);
+        return HPRQP_STATUS_NOT_IMPLEMENTED;
+    };
+    cudaError_t ce = cudaMemsetAsync(d_logn, 0, sizeof(int), b->stream);
+    if (ce != cudaSuccess) return cuda_fail(ce, __LINE__);
+    G.time_from_loop = 1;
+    G.iter4_out = d_i4;
+    G.iter6_out = d_i6;
+    G.time4_out = d_t;
+    G.time6_out = d_t + 1;
+    G.loop_seconds_out = d_t + 2;
+    G.log_buf = d_log;
+    G.log_cap = (int)cap;
+    G.log_count = d_logn;
+    HPRQPBatchParams bp;
+    hprqp_batch_params_set_defaults(&bp);
+    bp.stoptol = params->stoptol;
+    bp.max_iter = params->max_iter;
+    bp.time_limit = params->time_limit;
+    bp.check_iter = params->check_iter;
+    bp.print_frequency = params->print_frequency;
+    bp.use_scaling = params->use_scaling;
+    bp.device_number = params->device_number;
+    st = hprqp_batch_solve(b, &bp);
+    if (st != HPRQP_STATUS_OK) {
+        hprqp_batch_destroy(b);
+        return st;
+    }
+    int status = 0;
+    size_t iter = 0;
+    double pobj = 0.0, resid = 0.0, gap = 0.0;
+    results->x = (double *)calloc(n, sizeof(double));
+    results->w = (double *)calloc(n, sizeof(double));
+    results->z = (double *)calloc(n, sizeof(double));
+    results->y = m ? (double *)calloc(m, sizeof(double)) : nullptr;
+    if (!results->x || !results->w || !results->z || (m && !results->y)) {
+        results_free(results);
+        hprqp_batch_destroy(b);
+        return HPRQP_STATUS_ALLOCATION_FAILED;
+    }
+    st = hprqp_batch_get_results(b, &status, &iter, &pobj, &resid, &gap, results->x, results->y, results->z,
+                                 results->w);
+    long long i4 = -1, i6 = -1;
+    double t[3] = {0.0, 0.0, 0.0};
+    int nlog = 0;
+    if (st == HPRQP_STATUS_OK) {
+        if ((ce = cudaMemcpy(&i4, d_i4, sizeof(i4), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+            (ce = cudaMemcpy(&i6, d_i6, sizeof(i6), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+            (ce = cudaMemcpy(t, d_t, sizeof(t), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+            (ce = cudaMemcpy(&nlog, d_logn, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+            (nlog > 0 && (ce = cudaMemcpy(log_records, d_log, (size_t)nlog * kLogFields * sizeof(double),
+                                          cudaMemcpyDeviceToHost)) != cudaSuccess)) {
+            results_free(results);
+            return cuda_fail(ce, __LINE__);
+        }
+    }
+    hprqp_batch_destroy(b);
+    if (st != HPRQP_STATUS_OK) {
+        results_free(results);
+        return st;
+    }
+    if (log_count) *log_count = (size_t)nlog;
+    const double elapsed = t[2];
+    // the host loop's bookkeeping: a milestone never reached (or reached at
+    // iteration 0) reports the final iteration and time
+    results->iter = iter;
+    results->time = elapsed;
+    results->iter_4 = i4 <= 0 ? iter : (size_t)i4;
+    results->iter_6 = i6 <= 0 ? iter : (size_t)i6;
+    results->time_4 = (i4 < 0 || t[0] == 0.0) ? elapsed : t[0];
+    results->time_6 = (i6 < 0 || t[1] == 0.0) ? elapsed : t[1];
+    results->primal_obj = pobj;
+    results->residuals = resid;
+    results->gap = gap;
+    results->status = status;
+    return (HPRQPStatus)status;
+}
+
+}  // namespace hpr
+
+extern "C" size_t hprqp_b200_set_single_cta_max_work(size_t max_work)
+{
+    const size_t old = hpr::g_single_cta_max_work;
+    hpr::g_single_cta_max_work = max_work;
+    return old;
+}

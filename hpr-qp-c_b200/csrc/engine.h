@@ -61,6 +61,18 @@ HPRQPStatus engine_adjoint(Engine *e, const double *gx, const double *gy, double
 HPRQPStatus solve_gpu_keep(const HPRQPModel *model, const HPRQPParams *params, HPRQPResults *results,
                            Engine **keep);
 
+// Small single QPs: the whole solve in one CTA of the batch kernel (one
+// launch, no host round trips per iteration).  single_cta_eligible() says
+// whether solve_gpu takes this path for a model and parameters; the solve
+// fills results like the host loop (iterations, milestones, loop time,
+// objective, residuals, x, y, z, w) and, when log is given, appends one
+// record of 8 doubles per printed iteration (iter, errRp, errRd, primal obj,
+// dual obj, gap, sigma, loop seconds).
+constexpr size_t kSingleCtaLogCap = 100000;  // printed iterations the device log holds
+bool single_cta_eligible(const HPRQPModel *model, const HPRQPParams *params);
+HPRQPStatus solve_single_cta(const HPRQPModel *model, const HPRQPParams *params, HPRQPResults *results,
+                             double *log_records, size_t log_cap, size_t *log_count);
+
 // Kernel launch counter (process-wide, all engine kernels).
 uint64_t launch_count();
 void count_launch(uint64_t k = 1);

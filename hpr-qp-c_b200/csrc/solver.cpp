@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 namespace {
 
@@ -239,6 +240,32 @@ HPRQPStatus hpr::solve_gpu_keep(const HPRQPModel *model, const HPRQPParams *para
     if (params->verbose) {
         print_model_info(model);
         print_params_info(params);
+    }
+    if (!keep && hpr::single_cta_eligible(model, params)) {
+        // the whole solve in one CTA of the batch kernel; the log comes back
+        // with the results and is printed like the host loop prints it
+        std::vector<double> log;
+        if (params->verbose) log.resize(hpr::kSingleCtaLogCap * 8);
+        size_t nlog = 0;
+        const HPRQPStatus ret = hpr::solve_single_cta(model, params, results, params->verbose ? log.data() : nullptr,
+                                                      hpr::kSingleCtaLogCap, &nlog);
+        if (params->verbose && nlog > 0) {
+            printf("HPRQP SOLVER starts (GPU mode, sm_100a engine, one CTA)...\n");
+            printf(" iter     errRp        errRd         p_obj           d_obj          gap        sigma       time\n");
+            for (size_t i = 0; i < nlog; ++i) {
+                const double *r = log.data() + 8 * i;
+                HPRQPResiduals res;
+                memset(&res, 0, sizeof(res));
+                res.err_Rp_org_bar = r[1];
+                res.err_Rd_org_bar = r[2];
+                res.primal_obj_bar = r[3];
+                res.dual_obj_bar = r[4];
+                res.rel_gap_bar = r[5];
+                print_log((size_t)r[0], &res, r[6], r[7]);
+            }
+        }
+        results->total_time = now_s() - t_begin;
+        return ret;
     }
     hpr::Engine *eng = nullptr;
     hpr::SetupInfo info;

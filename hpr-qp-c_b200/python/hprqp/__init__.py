@@ -161,6 +161,8 @@ class _Library:
         lib.hprqp_b200_setup.argtypes = [ctypes.POINTER(_ModelStruct), ctypes.POINTER(_ParamsStruct)] + \
             [c_double_p] * 11
         lib.hprqp_b200_launch_count.restype = ctypes.c_uint64
+        lib.hprqp_b200_set_single_cta_max_work.argtypes = [ctypes.c_size_t]
+        lib.hprqp_b200_set_single_cta_max_work.restype = ctypes.c_size_t
         lib.params_set_defaults.argtypes = [ctypes.POINTER(_ParamsStruct)]
         lib.params_set_defaults.restype = None
 
@@ -184,6 +186,14 @@ def gpu_backend_available() -> bool:
 
 def launch_count() -> int:
     return int(_lib().hprqp_b200_launch_count())
+
+
+def set_single_cta_max_work(max_work: int) -> int:
+    """Route solve_gpu: models without cones whose products per iteration
+    touch at most ``max_work`` nonzeros (2 nnz(Q) + 2 nnz(A)) are solved in
+    one CTA of the batch kernel; 0 sends every model through the host-driven
+    loop.  Returns the previous value (hprqp_b200_set_single_cta_max_work)."""
+    return int(_lib().hprqp_b200_set_single_cta_max_work(int(max_work)))
 
 
 def _raise_for_status(code: int, context: str) -> int:

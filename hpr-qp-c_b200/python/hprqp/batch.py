@@ -50,6 +50,9 @@ def _configure():
     lib.hprqp_batch_last_backward_ms.restype = ctypes.c_double
     lib.hprqp_batch_destroy.argtypes = [vp]
     lib.hprqp_batch_destroy.restype = None
+    lib.hprqp_batch_set_spmv_lanes.argtypes = [vp, ctypes.c_int]
+    lib.hprqp_batch_request_abort.argtypes = [vp]
+    lib.hprqp_batch_get_spmv_lanes.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     _configured = True
 
 
@@ -217,6 +220,26 @@ class Batch:
         ptr = (lambda a: None if a is None else a.ctypes.data_as(c_double_p))
         _raise_for_status(_lib().hprqp_batch_set_warm_start(self._handle, ptr(x), ptr(y), ptr(w), ptr(sg)),
                           "hprqp_batch_set_warm_start")
+
+    def request_abort(self):
+        """Stop the solve running on this batch in another thread
+        (hprqp_batch_request_abort): unfinished instances end with
+        TIME_LIMIT (5)."""
+        _raise_for_status(_lib().hprqp_batch_request_abort(self._handle), "hprqp_batch_request_abort")
+
+    def spmv_lanes(self) -> np.ndarray:
+        """SpMV lane-group width of every matrix, shape (K, 3): Q, A, A'
+        (hprqp_batch_get_spmv_lanes)."""
+        out = np.zeros(3 * max(self.K, 1), np.int32)
+        _raise_for_status(_lib().hprqp_batch_get_spmv_lanes(self._handle,
+                                                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_int))),
+                          "hprqp_batch_get_spmv_lanes")
+        return out[:3 * self.K].reshape(self.K, 3)
+
+    def set_spmv_lanes(self, lanes: int = 0):
+        """Force one SpMV lane-group width (1, 2, 4, 8, 16, 32) on every
+        matrix; 0 restores the autotuned widths (hprqp_batch_set_spmv_lanes)."""
+        _raise_for_status(_lib().hprqp_batch_set_spmv_lanes(self._handle, int(lanes)), "hprqp_batch_set_spmv_lanes")
 
     def solve(self, **kw) -> float:
         params = default_params(**kw)

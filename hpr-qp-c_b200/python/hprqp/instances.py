@@ -168,6 +168,30 @@ def config1(instance: int = 0, scale: float = 1.0) -> QPInstance:
     return QPInstance(Qc, A, cvec, AL, AU, np.full(n, -10.0), np.full(n, 10.0), 0.0, "config1")
 
 
+def config1_sized_plain(instance: int = 0, scale: float = 1.0) -> QPInstance:
+    """The plain recipe (uniform A pattern, Q = M'M + 0.01 I, x in [-10, 10],
+    40% equality rows) at the large QP's sizes: n=1e6, m=5e5, nnz(A)=1e7,
+    M 2e5 x 1e6 with 2.5e6 nnz (nnz(Q) ~ 3.2e7).  Used for the single large
+    backward, whose forward solve must reach its tolerance.  Positions are
+    drawn with replacement and duplicates dropped (a few per million)."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(SEED_BASE + 5000 + instance)
+    n = int(round(1_000_000 * scale))
+    m = int(round(500_000 * scale))
+    nnz_a = int(round(10_000_000 * scale))
+    key = np.unique(rng.integers(0, m, nnz_a, dtype=np.int64) * n + rng.integers(0, n, nnz_a, dtype=np.int64))
+    A = _csr_from_coo(m, n, key // n, key % n, rng.standard_normal(len(key)))
+    kb = int(round(200_000 * scale))
+    nnz_b = int(round(2_500_000 * scale))
+    bkey = np.unique(rng.integers(0, kb, nnz_b, dtype=np.int64) * n + rng.integers(0, n, nnz_b, dtype=np.int64))
+    M = sp.csr_matrix((rng.standard_normal(len(bkey)), (bkey // n, bkey % n)), shape=(kb, n))
+    Q = _csr_from_scipy((M.T @ M).tocsr() + 0.01 * sp.identity(n, format="csr"))
+    cvec = rng.standard_normal(n)
+    AL, AU = _feasible_rows(rng, A, n, int(0.4 * m))
+    return QPInstance(Q, A, cvec, AL, AU, np.full(n, -10.0), np.full(n, 10.0), 0.0, "config1_sized_plain")
+
+
 def config2(instance: int = 0, n_assets: int = 200_000, k: int = 200, sectors: int = 500) -> QPInstance:
     """Factor-structured portfolio QP with variables (x, f), f = F'x."""
     rng = np.random.default_rng(SEED_BASE + 2000 + instance)

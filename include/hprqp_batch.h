@@ -68,6 +68,19 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *batch, const HPRQPBatchParams *params)
 HPRQPStatus hprqp_batch_set_warm_start(HPRQPBatch *batch, const double *x0, const double *y0, const double *w0,
                                        const double *sigma0);
 
+/* Ask the hprqp_batch_solve running on this batch (from another host
+ * thread) to stop early -- an addition; the reference's only stop besides
+ * convergence and max_iter is its time limit (src/shared/solver_backend.c:
+ * 432-513), and an aborted instance ends the same way: an instance being
+ * solved stops within 16 iterations with HPRQP_STATUS_TIME_LIMIT and its
+ * current iterates, residuals recomputed; an instance not started yet (also
+ * one started after time_limit has passed) is not set up and reports
+ * HPRQP_STATUS_TIME_LIMIT at iteration 0 with zero vectors and infinite
+ * residual and gap.  The solve then returns HPRQP_STATUS_OK as usual.  The
+ * request stays set until a solve has ended, so a request made just before
+ * hprqp_batch_solve starts stops that solve. */
+HPRQPStatus hprqp_batch_request_abort(HPRQPBatch *batch);
+
 /* sigma of each instance at the end of the last hprqp_batch_solve. */
 HPRQPStatus hprqp_batch_get_sigma(const HPRQPBatch *batch, double *sigma);
 
@@ -76,6 +89,20 @@ HPRQPStatus hprqp_batch_get_sigma(const HPRQPBatch *batch, double *sigma);
  * concurrently, so these do not add up to the launch time).  The per-solve
  * time a dataset table reports for a batched run. */
 HPRQPStatus hprqp_batch_get_times(const HPRQPBatch *batch, double *seconds);
+
+/* SpMV lane-group width of every matrix (an addition; the reference picks
+ * between cuSPARSE and its own kernel per matrix by timing them,
+ * src/gpu/iteration.cu:1287-1382).  Inside the solve kernel each row of Q,
+ * A and A' is summed by a group of 1, 2, 4, 8, 16 or 32 lanes; by default
+ * the width of each matrix of each instance is chosen when the batch is
+ * created, from that matrix's row lengths (a cost model of the rounds,
+ * passes and shuffles of the product).  hprqp_batch_set_spmv_lanes(b, w)
+ * forces width w on every matrix (w = 0 restores the chosen widths; other
+ * values: HPRQP_STATUS_INVALID_ARGUMENT); every width gives the same
+ * iterates up to rounding.  hprqp_batch_get_spmv_lanes writes 3 widths per
+ * instance (Q, A, A') in instance order. */
+HPRQPStatus hprqp_batch_set_spmv_lanes(HPRQPBatch *batch, int lanes);
+HPRQPStatus hprqp_batch_get_spmv_lanes(const HPRQPBatch *batch, int *lanes);
 
 /* Device time of the last hprqp_batch_solve kernel, milliseconds. */
 double hprqp_batch_last_solve_ms(const HPRQPBatch *batch);

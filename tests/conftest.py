@@ -33,3 +33,14 @@ def engine_lib():
     import hprqp
 
     return hprqp
+
+
+@pytest.fixture(params=["host_loop", "single_cta"])
+def plain_path(request, engine_lib):
+    """Runs a plain-path test through both routes of solve_gpu: the
+    host-driven loop of fused device passes, and the whole solve in one CTA
+    of the batch kernel (hprqp_b200_set_single_cta_max_work)."""
+    big = 1 << 40
+    old = engine_lib.set_single_cta_max_work(0 if request.param == "host_loop" else big)
+    yield request.param
+    engine_lib.set_single_cta_max_work(old)

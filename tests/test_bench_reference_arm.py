@@ -32,3 +32,16 @@ def test_reference_arm_json_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and "sample" in cb
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_objective_agreement_counts_only_both_optimal():
+    sys.path.insert(0, str(ROOT))
+    import numpy as np
+
+    import bench
+
+    got = bench.objective_agreement(np.array([6, 6, 4]), np.array([1.0, -2.0, 3.0]),
+                                    [(0, 6, 1.0 + 1e-7), (1, 6, -2.0), (2, 6, 30.0)])
+    assert got["instances"] == 3 and got["both_optimal"] == 2
+    assert abs(got["max_rel_objective_diff"] - 1e-7) < 1e-12
+    assert bench.objective_agreement(np.array([4]), np.array([0.0]), [(0, 6, 1.0)])["max_rel_objective_diff"] is None

@@ -72,6 +72,47 @@ def test_batch_steps_within_reference_iteration_tolerance(engine_lib, cap):
             assert len(ref) == 0 or np.max(np.abs(got - ref)) <= 1e-12, inst.name
 
 
+@pytest.mark.parametrize("lanes", [0, 1, 2, 4, 8, 16, 32])
+@pytest.mark.parametrize("cap", [1, 10])
+def test_batch_spmv_lane_widths(engine_lib, lanes, cap):
+    """Every SpMV lane-group width the autotuner can pick (forced on every
+    matrix of every instance; 0 = the autotuned widths) gives the oracle's
+    status and iteration count and its iterates within the reference's
+    1e-12 step tolerance (tests/gpu/test_gpu_iteration.cpp:42-90), relative
+    to the iterate's scale, on the fixture models and batch-recipe QPs."""
+    from hprqp import batch
+
+    insts = instances.tiny_cases() + [instances.config3_instance(i) for i in (1, 7, 12)]
+    b = batch.Batch(insts)
+    tuned = b.spmv_lanes()
+    assert set(np.unique(tuned)) <= {1, 2, 4, 8, 16, 32}
+    b.set_spmv_lanes(lanes)
+    if lanes:
+        assert np.all(b.spmv_lanes() == lanes)
+    else:
+        assert np.array_equal(b.spmv_lanes(), tuned)
+    b.solve(stoptol=1e-8, max_iter=cap)
+    r = b.results()
+    b.close()
+    xs, ys, zs, ws = b.split(r.x, "x"), b.split(r.y, "y"), b.split(r.z, "x"), b.split(r.w, "x")
+    for k, inst in enumerate(insts):
+        o = pyoracle.OracleModel(inst).solve(stoptol=1e-8, max_iter=cap, mode=pyoracle.MODE_GPU_REF)
+        assert r.status[k] == o["status"] and r.iter[k] == o["iter"], (inst.name, lanes)
+        for got, ref in ((xs[k], o["x"]), (ys[k][_kept(inst)], o["y"]), (zs[k], o["z"]), (ws[k], o["w"])):
+            if len(ref):
+                assert np.max(np.abs(got - ref)) <= 1e-12 * max(1.0, float(np.max(np.abs(ref)))), (inst.name, lanes)
+
+
+def test_batch_spmv_lanes_rejects_bad_width(engine_lib):
+    from hprqp import batch
+
+    b = batch.Batch(instances.tiny_cases()[:2])
+    for bad in (3, 64, -1):
+        with pytest.raises(Exception):
+            b.set_spmv_lanes(bad)
+    b.close()
+
+
 def test_batch_tiny_converge(engine_lib):
     from hprqp import batch
 

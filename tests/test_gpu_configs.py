@@ -1,0 +1,79 @@
+"""The plain solve on the large workloads, against the reference's own GPU
+build (oracle/_ref/libhprqp_ref_gpu.so: cuSPARSE SpMV, cuBLAS reductions,
+polishing 0, Gram off) and the CPU oracle, with the reference's end-to-end
+bar (tests/gpu/test_gpu_solver.c:73-81: objective and residuals agree, both
+reach the tolerance) and the KKT residual recomputed in FP64 on the host from
+the original model.
+
+* the factor-structured portfolio QP at full size (n=200,200, 200 dense
+  factor rows of 200,001 entries, diagonal Q), stoptol 1e-6;
+* the large power-law QP recipe shrunk to 1% and 10% of its dimensions
+  (n = 1e4 and 1e5), stoptol 1e-8;
+* the large power-law QP at full size (n=1e6, m=5e5, nnz(A)=1e7,
+  nnz(Q)=3.2e7) for fixed iteration budgets of 200 and 1000 iterations:
+  both solvers stop at MAX_ITER; their KKT residuals and objectives agree
+  within the drift of two FP64 trajectories whose SpMVs round differently.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import pyoracle
+from hprqp import instances
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not pyoracle.ref_gpu_available(),
+                                 reason="reference GPU library not built (make -C oracle ref-gpu)")]
+
+
+def _ours(hprqp, inst, stoptol, max_iter=2147483647):
+    model = hprqp.build_from_instance(inst)
+    return hprqp.optimize(model, hprqp.Parameters(verbose=False, stoptol=stoptol, max_iter=max_iter,
+                                                  time_limit=600.0), as_numpy=True)
+
+
+def _rel(a, b):
+    return abs(a - b) / max(1.0, abs(b))
+
+
+def test_portfolio_full_size_matches_reference_gpu(engine_lib):
+    inst = instances.config2()
+    ref = pyoracle.RefGpuModel(inst).solve(stoptol=1e-6)
+    assert ref["status"] == engine_lib.STATUS_OPTIMAL
+    r = _ours(engine_lib, inst, 1e-6)
+    assert r.status_code == engine_lib.STATUS_OPTIMAL
+    assert _rel(r.objective, ref["primal_obj"]) <= 1e-6, (r.objective, ref["primal_obj"])
+    om = pyoracle.OracleModel(inst)
+    assert om.kkt(r.x, r.y, r.z)["kkt"] <= 1.01e-6
+    assert om.kkt(ref["x"], ref["y"], ref["z"])["kkt"] <= 1.01e-6
+
+
+@pytest.mark.parametrize("scale", [0.01, 0.1])
+def test_large_qp_scaled_matches_reference_gpu_and_oracle(engine_lib, scale):
+    inst = instances.config1(scale=scale)
+    ref = pyoracle.RefGpuModel(inst).solve(stoptol=1e-8)
+    assert ref["status"] == engine_lib.STATUS_OPTIMAL
+    r = _ours(engine_lib, inst, 1e-8)
+    assert r.status_code == engine_lib.STATUS_OPTIMAL
+    assert _rel(r.objective, ref["primal_obj"]) <= 1e-6, (r.objective, ref["primal_obj"])
+    om = pyoracle.OracleModel(inst)
+    assert om.kkt(r.x, r.y, r.z)["kkt"] <= 1.01e-8
+    if scale <= 0.01:  # the serial oracle solves n = 1e4 in seconds
+        o = om.solve(stoptol=1e-8, mode=pyoracle.MODE_GPU_REF)
+        assert o["status"] == engine_lib.STATUS_OPTIMAL
+        assert _rel(r.objective, o["primal_obj"]) <= 1e-6
+        assert abs(int(r.iter) - o["iter"]) <= max(20, o["iter"] // 10), (r.iter, o["iter"])
+
+
+@pytest.mark.parametrize("budget", [200, 1000])
+def test_large_qp_full_size_fixed_budget_matches_reference_gpu(engine_lib, budget):
+    inst = instances.config1()
+    ref = pyoracle.RefGpuModel(inst).solve(stoptol=1e-8, max_iter=budget)
+    r = _ours(engine_lib, inst, 1e-8, max_iter=budget)
+    assert r.status_code == ref["status"] == engine_lib.STATUS_MAX_ITER
+    assert int(r.iter) == ref["iter"] == budget
+    # same trajectory up to rounding drift: the KKT residuals within 5% of
+    # each other and the objectives within 1e-3 relative after the budget
+    assert abs(r.residual - ref["residuals"]) <= 0.05 * ref["residuals"], (r.residual, ref["residuals"])
+    assert _rel(r.objective, ref["primal_obj"]) <= 1e-3, (r.objective, ref["primal_obj"])

@@ -186,7 +186,7 @@ TINY = [i for i in instances.tiny_cases()]
 
 @pytest.mark.parametrize("inst", TINY, ids=[i.name for i in TINY])
 @pytest.mark.parametrize("cap", [1, 10, 100, 250])
-def test_iterates_after_k_steps(engine_lib, inst, cap):
+def test_iterates_after_k_steps(engine_lib, plain_path, inst, cap):
     r, o = _solve_pair(engine_lib, inst, stoptol=1e-8, max_iter=cap)
     assert r.status_code == o["status"]
     assert r.iter == o["iter"]
@@ -196,7 +196,7 @@ def test_iterates_after_k_steps(engine_lib, inst, cap):
 
 @pytest.mark.parametrize("inst", TINY, ids=[i.name for i in TINY])
 @pytest.mark.parametrize("cap", [1, 10])
-def test_steps_within_reference_iteration_tolerance(engine_lib, inst, cap):
+def test_steps_within_reference_iteration_tolerance(engine_lib, plain_path, inst, cap):
     """the reference's GPU-vs-CPU step tolerance, 1e-12 absolute
     (tests/gpu/test_gpu_iteration.cpp:42-90), on the whole solve after 1
     and 10 steps (setup, scaling and power iterations included); measured
@@ -210,14 +210,14 @@ def test_steps_within_reference_iteration_tolerance(engine_lib, inst, cap):
 
 @pytest.mark.parametrize("inst", [i for i in TINY if i.name != "tall_diag"],
                          ids=[i.name for i in TINY if i.name != "tall_diag"])
-def test_tiny_solves_converge_like_oracle(engine_lib, inst):
+def test_tiny_solves_converge_like_oracle(engine_lib, plain_path, inst):
     r, o = _solve_pair(engine_lib, inst, stoptol=1e-8)
     assert r.status_code == o["status"] == engine_lib.STATUS_OPTIMAL
     assert abs(r.objective - o["primal_obj"]) <= 1e-6 * max(1.0, abs(o["primal_obj"]))
     assert abs(r.iter - o["iter"]) <= max(10, o["iter"] // 10)
 
 
-def test_config0_end_to_end(engine_lib):
+def test_config0_end_to_end(engine_lib, plain_path):
     """n=1000, m=500 seeded QP at 1e-6: same tolerance reached, objective
     within 1e-6 relative, KKT recomputed on the host in FP64."""
     inst = instances.config0()
@@ -229,7 +229,32 @@ def test_config0_end_to_end(engine_lib):
     assert abs(r.iter - o["iter"]) <= max(20, o["iter"] // 10)
 
 
-def test_reference_python_api_gpu_path(engine_lib):
+def test_single_cta_route_keeps_host_loop_bookkeeping(engine_lib, capfd):
+    """The one-CTA route of solve_gpu reports what the host loop reports:
+    status, iterations, the 1e-4 / 1e-6 milestones, and (verbose) the same
+    printed iterations of the residual log."""
+    hprqp = engine_lib
+    model = hprqp.build_from_instance(instances.config0())
+    out = {}
+    for route, work in (("host_loop", 0), ("single_cta", 1 << 40)):
+        old = hprqp.set_single_cta_max_work(work)
+        try:
+            capfd.readouterr()
+            r = hprqp.optimize(model, hprqp.Parameters(verbose=True, stoptol=1e-6), as_numpy=True)
+            text = capfd.readouterr().out
+        finally:
+            hprqp.set_single_cta_max_work(old)
+        iters = [int(line.split()[0]) for line in text.splitlines()
+                 if line.strip() and line.split()[0].isdigit() and len(line.split()) == 8]
+        out[route] = (r, iters)
+    (a, ia), (b, ib) = out["host_loop"], out["single_cta"]
+    assert a.status_code == b.status_code == hprqp.STATUS_OPTIMAL
+    assert a.iter == b.iter and a.iter_4 == b.iter_4 and a.iter_6 == b.iter_6
+    assert ia == ib and ia[0] == 0 and ia[-1] == a.iter
+    assert 0.0 < b.time_4 <= b.time_6 <= b.time
+
+
+def test_reference_python_api_gpu_path(engine_lib, plain_path):
     """python/tests/test_hprqp.py:44-65 of the reference, GPU side."""
     hprqp = engine_lib
     assert hprqp.gpu_backend_available()
@@ -246,7 +271,7 @@ def test_reference_python_api_gpu_path(engine_lib):
     assert r2.y == []
 
 
-def test_max_iter_zero_and_invalid_device(engine_lib):
+def test_max_iter_zero_and_invalid_device(engine_lib, plain_path):
     hprqp = engine_lib
     model = hprqp.build_from_instance(TINY[0])
     r = hprqp.optimize(model, hprqp.Parameters(verbose=False, max_iter=0))
@@ -289,7 +314,7 @@ def test_residual_kernels_match_oracle(engine_lib, scaling):
         assert abs(r[key] - k[key]) <= 1e-10 * max(1.0, abs(k[key])), (key, r[key], k[key])
 
 
-def test_reference_mps_fixture_through_binding(engine_lib):
+def test_reference_mps_fixture_through_binding(engine_lib, plain_path):
     """tests/test_binding_api.c:16-118 of the reference on its own
     simple_qp.mps: 2 variables and 2 rows, max_iter 0 gives MAX_ITER with
     solution vectors; solved to 1e-8 it matches the reference CPU solver's
