@@ -695,8 +695,22 @@ def main():
         for mdl in models:
             hprqp.optimize(mdl, params)
         plain_rate = len(models) / (time.perf_counter() - t0)
-        line["plain"] = {"value": plain_rate, "unit": "solves/s", "sample": f"{len(models)} instances of the batch"}
+        # the same loop through the host-driven route of solve_gpu (every
+        # iteration launched from the host), which small QPs no longer take
+        old_route = hprqp.set_single_cta_max_work(0)
+        try:
+            hprqp.optimize(models[0], params)
+            t0 = time.perf_counter()
+            for mdl in models:
+                hprqp.optimize(mdl, params)
+            host_loop_rate = len(models) / (time.perf_counter() - t0)
+        finally:
+            hprqp.set_single_cta_max_work(old_route)
+        line["plain"] = {"value": plain_rate, "unit": "solves/s", "sample": f"{len(models)} instances of the batch",
+                         "route": "one CTA of the batch kernel per solve_gpu call (small models)",
+                         "host_loop": host_loop_rate}
         line["batched_over_plain"] = value / world / plain_rate
+        line["batched_over_plain_host_loop"] = value / world / host_loop_rate
         if not args.no_spmv:
             line["spmv"] = spmv_leg(peak)
         if not args.no_adjoint:

@@ -124,7 +124,9 @@ def test_batch_tiny_converge(engine_lib):
 
 
 def test_batch_seeded_matches_oracle_and_plain(engine_lib):
-    """Instances of the 4096-QP recipe: batch == plain solve == oracle."""
+    """Instances of the 4096-QP recipe: batch == plain solve == oracle (the
+    plain solve through the host-driven loop, not the one-CTA route, which
+    runs the batch kernel itself)."""
     hprqp = engine_lib
     from hprqp import batch
 
@@ -142,7 +144,11 @@ def test_batch_seeded_matches_oracle_and_plain(engine_lib):
         assert abs(int(r.iter[k]) - o["iter"]) <= max(20, o["iter"] // 10), (k, r.iter[k], o["iter"])
         kkt = om.kkt(xs[k], ys[k][_kept(inst)], zs[k])["kkt"]
         assert kkt <= 1.01e-6, (k, kkt)
-        p = hprqp.optimize(hprqp.build_from_instance(inst), hprqp.Parameters(verbose=False, stoptol=1e-6))
+        old = hprqp.set_single_cta_max_work(0)
+        try:
+            p = hprqp.optimize(hprqp.build_from_instance(inst), hprqp.Parameters(verbose=False, stoptol=1e-6))
+        finally:
+            hprqp.set_single_cta_max_work(old)
         assert abs(p.objective - r.objective[k]) <= 1e-6 * abs(p.objective)
 
 
