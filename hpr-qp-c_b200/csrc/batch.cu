@@ -13,15 +13,15 @@
 //
 // Inside a CTA, y = M x gives every warp a contiguous range of rows and
 // runs it as a CSR-vector product: a group of g lanes shares a row (32/g
-// rows per pass), each lane issues kU independent index/value loads per
-// round, and the group folds its partial sums with g-1 shuffles.  The group
-// width g of each matrix (Q, A, A') of each instance is chosen on the host
-// when the batch is packed, from that matrix's sequence of row lengths, by a
-// cost model of the rounds, passes and shuffles every warp would run (the
-// per-instance SpMV autotuner, choose_lane_group).  The choice is structural,
-// so an instance sums in the same order in every solve; every reduction is
-// folded in a fixed order, so each instance's result is independent of which
-// CTA solved it.
+// rows per pass), each lane reads the row as 16-byte-aligned quads of
+// entries, and the group folds its partial sums with g-1 shuffles.  The
+// group width g of each matrix (Q, A, A') of each instance is chosen on the
+// host when the batch is packed, from that matrix's sequence of row
+// lengths, by a cost model of the rounds, passes and shuffles every warp
+// would run (the per-instance SpMV autotuner, choose_lane_group).  The choice
+// is structural, so an instance sums in the same order in every solve; every
+// reduction is folded in a fixed order, so each instance's result is
+// independent of which CTA solved it.
 #include "engine.h"
 #include "hprqp_batch.h"
 #include "hprqp.h"
@@ -41,12 +41,12 @@
 
 namespace hpr {
 
-// 512 threads, two CTAs (two instances) per SM: one instance's barrier and
-// gather stalls overlap the other's.  Measured on the 4096-QP batch: 740
-// solves/s, against 679 for 1024 threads with the vectors in shared memory
-// and 627 for 256 threads x 4 CTAs.
+// 1024 threads, one CTA (one instance) per SM.  Measured on the 4096-QP
+// batch with the quad-load SpMV: 865 solves/s, against 779 for 512 threads
+// x 2 CTAs per SM; 148 instances in flight keep more of their matrices in
+// L2 than 296, and each instance gets twice the warps.
 #ifndef HPR_BATCH_THREADS
-#define HPR_BATCH_THREADS 512
+#define HPR_BATCH_THREADS 1024
 #endif
 #ifndef HPR_BATCH_LD
 #define HPR_BATCH_LD __ldg  // instance matrices are re-read every iteration: keep them in L2
@@ -54,16 +54,13 @@ namespace hpr {
 #ifndef HPR_BATCH_VEC_SMEM
 #define HPR_BATCH_VEC_SMEM 1
 #endif
-#ifndef HPR_BATCH_U
-#define HPR_BATCH_U 4
-#endif
 constexpr int kBT = HPR_BATCH_THREADS;  // threads per CTA of the batch kernel
 constexpr int kBW = kBT / 32;
-constexpr int kU = HPR_BATCH_U;  // independent index/value loads per lane per round of the SpMV
-// dynamic shared memory per CTA: half an SM, so that two CTAs fit; the
-// gathered vectors move to shared memory when they fit (every instance of
-// n, m <= 2000), else they stay in global memory (L1-cached)
-constexpr size_t kSmemLimit = 110 * 1024;
+constexpr int kCtasPerSm = kBT >= 1024 ? 1 : 1024 / kBT;
+// dynamic shared memory per CTA: the gathered vectors and the SpMV row-sum
+// arrays move to shared memory when they fit (every instance of n, m <=
+// 2000 at one CTA per SM), else they stay in global memory (L1-cached)
+constexpr size_t kSmemLimit = kCtasPerSm == 1 ? 200 * 1024 : 110 * 1024;
 
 struct BInst {
     long long q_nz, a_nz, at_nz;  // first entry of the instance's matrices
@@ -195,8 +192,9 @@ __device__ __forceinline__ void cta_allreduce(double (&v)[N], const int (&ops)[N
 }
 
 // Rows of a matrix with nrow rows that warp `warp` owns in cta_spmv: one
-// contiguous range per warp.  It depends on nrow only, so products with Q
-// and A' (both n rows) call their epilogues for a row on the same thread.
+// contiguous range per warp, balanced to within one row.  It depends on
+// nrow only, so products with Q and A' (both n rows) call their epilogues
+// for a row on the same thread.
 __device__ __forceinline__ void warp_rows(int nrow, int warp, int &r0, int &r1)
 {
     const int per = (nrow + kBW - 1) / kBW;
@@ -209,17 +207,22 @@ __device__ __forceinline__ void warp_rows(int nrow, int warp, int &r0, int &r1)
 //
 // Each warp walks its rows in chunks of 32: the chunk's row pointers are
 // read once (one per lane), then passes of 32/g rows run with g lanes per
-// row.  In a round every lane of a group loads kU entries of its row (lane
-// j of the group takes entries j, j+g, ..., all loads issued before the
-// gathers), multiplies them into its own sum in entry order; the group then
-// folds its g sums with an xor-shuffle tree and the row's value moves to
-// the lane that owns the row.  The summation order depends on g only.
+// row.  A row's entries are read as 16-byte-aligned quads (one int4 of
+// column indices and two double2 of values; every instance's entries start
+// on a 4-entry boundary and the arrays carry 4 entries of tail padding):
+// lane j of the group takes quads j, j+g, ... of the aligned span that
+// covers the row, masks the entries outside the row, and adds v * x[col]
+// into its own sum in entry order.  The group folds its g sums with an
+// xor-shuffle tree and the row's value moves to the lane that owns the row.
+// The summation order depends on g only.
 template <class F>
 __device__ __forceinline__ void cta_spmv(const LCsr &M, const double *x, F &&f)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lg = M.lg, g = 1 << lg, sh = 5 - lg, rpp = 32 >> lg;
     const int gl = lane & (g - 1), grp = lane >> lg;
+    const int4 *ci4 = reinterpret_cast<const int4 *>(M.ci);
+    const double2 *v2 = reinterpret_cast<const double2 *>(M.v);
     int w0, w1;
     warp_rows(M.nrow, warp, w0, w1);
     for (int c0 = w0; c0 < w1; c0 += 32) {
@@ -234,18 +237,22 @@ __device__ __forceinline__ void cta_spmv(const LCsr &M, const double *x, F &&f)
             const int e = __shfl_sync(0xffffffffu, my_e, rr);
             double s = 0.0;
             if (rr < nr) {
-                for (int k = b + gl; k < e; k += g * kU) {
-                    int c[kU];
-                    double v[kU];
-#pragma unroll
-                    for (int u = 0; u < kU; ++u) {
-                        const int kk = k + u * g;
-                        c[u] = kk < e ? HPR_BATCH_LD(M.ci + kk) : 0;
-                        v[u] = kk < e ? HPR_BATCH_LD(M.v + kk) : 0.0;
+                const int q1 = (e + 3) >> 2;
+                for (int q = (b >> 2) + gl; q < q1; q += g) {
+                    const int4 c = HPR_BATCH_LD(ci4 + q);
+                    const double2 va = HPR_BATCH_LD(v2 + 2 * q), vb = HPR_BATCH_LD(v2 + 2 * q + 1);
+                    const int k0 = 4 * q;
+                    if (k0 >= b && k0 + 4 <= e) {  // a quad inside the row
+                        s = fma(va.x, x[c.x], s);
+                        s = fma(va.y, x[c.y], s);
+                        s = fma(vb.x, x[c.z], s);
+                        s = fma(vb.y, x[c.w], s);
+                    } else {  // the first or last quad of the row
+                        if (k0 >= b && k0 < e) s = fma(va.x, x[c.x], s);
+                        if (k0 + 1 >= b && k0 + 1 < e) s = fma(va.y, x[c.y], s);
+                        if (k0 + 2 >= b && k0 + 2 < e) s = fma(vb.x, x[c.z], s);
+                        if (k0 + 3 >= b && k0 + 3 < e) s = fma(vb.y, x[c.w], s);
                     }
-#pragma unroll
-                    for (int u = 0; u < kU; ++u)
-                        if (k + u * g < e) s = fma(v[u], x[c[u]], s);
                 }
             }
             for (int o = g >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -336,8 +343,8 @@ __device__ __forceinline__ double row_abs(const LCsr &M, int r, bool sum)
 }
 
 // Power iteration (reference src/gpu/eigs.cu:185-383), CTA-wide.
-static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q, bool is_a, int len, double *z, double *q,
-                            double *tmp, double (*s_red)[8], double *s_out)
+static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q, bool is_a, int len, double *z,
+                            double *q, double *tmp, double (*s_red)[8], double *s_out)
 {
     if (len == 0) return 0.0;
     const int tid = threadIdx.x;
@@ -400,7 +407,29 @@ static __device__ __forceinline__ size_t adaptive_step_d(long long iter)
     return step;
 }
 
-__global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs B)
+// a % d == 0 for the iteration counters of thread 0, in 32-bit arithmetic
+// while both fit (every practical count; 64-bit division is a long software
+// sequence that the whole CTA would wait for at the next barrier)
+static __device__ __forceinline__ bool divides(long long a, long long d)
+{
+    if (a >= 0 && d > 0 && a <= 0x7fffffffLL && d <= 0x7fffffffLL) return (unsigned)a % (unsigned)d == 0u;
+    return a % d == 0;
+}
+
+// iter lies on the reference's adaptive print grid (src/shared/solver_backend.c
+// print steps: every 10 below 1000, every 100 below 10000, ...)
+static __device__ __forceinline__ bool on_print_grid(long long iter)
+{
+    if (iter >= 0 && iter <= 0x7fffffffLL) {
+        const unsigned it = (unsigned)iter;
+        unsigned step = 10;
+        while (it / step >= 100u && step <= 100000000u) step *= 10;
+        return it % step == 0u;
+    }
+    return iter % (long long)adaptive_step_d(iter) == 0;
+}
+
+__global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs B)
 {
     extern __shared__ __align__(16) double dyn_smem[];
     __shared__ CtaState S;
@@ -418,8 +447,10 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             // an instance taken after the batch's time limit or after an
             // abort request is not set up: it reports TIME_LIMIT at iteration
             // 0 with zero vectors and infinite residuals
+            // (a single-QP solve counts its time limit from its own loop)
             s_skip = s_inst >= 0 && (abort_requested(B.abort_flag) ||
-                                     1e-9 * (double)(globaltimer_ns() - B.t_start) > B.time_limit);
+                                     (!B.time_from_loop &&
+                                      1e-9 * (double)(globaltimer_ns() - B.t_start) > B.time_limit));
         }
         __syncthreads();
         const int k = s_inst;
@@ -1047,12 +1078,12 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
                 int print_yes = 0;
                 if (iter > 0) {
                     if (B.print_frequency == -1 &&
-                        ((long long)(iter % (long long)adaptive_step_d(iter)) == 0 || iter == B.max_iter || over))
+                        (on_print_grid(iter) || iter == B.max_iter || over))
                         print_yes = 1;
-                    if (B.print_frequency > 0 && (iter % B.print_frequency == 0 || iter == B.max_iter || over))
+                    if (B.print_frequency > 0 && (divides(iter, B.print_frequency) || iter == B.max_iter || over))
                         print_yes = 1;
                 }
-                S.do_res = iter > 0 && ((B.check_iter > 0 && iter % B.check_iter == 0) || print_yes);
+                S.do_res = iter > 0 && ((B.check_iter > 0 && divides(iter, B.check_iter)) || print_yes);
                 S.print_yes = print_yes;
                 S.scal[1] = el;
             }
@@ -1084,7 +1115,7 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
                             S.best_gap = S.current_gap;
                             S.best_sigma = S.sigma;
                         }
-                    } else if (iter % ci == 0) {
+                    } else if (divides(iter, ci)) {
                         if (S.current_gap < 0.0) S.current_gap = 1e-6;
                         if (S.current_gap <= 0.2 * S.last_gap) S.restart_flag = 1;
                         if (S.current_gap <= 0.8 * S.last_gap && S.current_gap > S.save_gap) S.restart_flag = 2;
@@ -1110,16 +1141,16 @@ __global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_solve(const BatchArgs
             if (tid == 0) {
                 const long long nx = iter + 1;
                 int t = 0;
-                if (B.check_iter > 0 && nx % B.check_iter == 0) t = 1;
+                if (B.check_iter > 0 && divides(nx, B.check_iter)) t = 1;
                 if (S.restart_flag > 0) t = 1;
-                if (B.print_frequency == -1 && nx % (long long)adaptive_step_d(nx) == 0) t = 1;
-                if (B.print_frequency > 0 && nx % B.print_frequency == 0) t = 1;
+                if (B.print_frequency == -1 && on_print_grid(nx)) t = 1;
+                if (B.print_frequency > 0 && divides(nx, B.print_frequency)) t = 1;
                 S.to_check = t;
             }
             __syncthreads();
             step(S.to_check);
             PHASE_ADD(3);
-            const bool at_check = B.check_iter > 0 && (iter + 1) % B.check_iter == 0;
+            const bool at_check = B.check_iter > 0 && divides(iter + 1, B.check_iter);
             if (S.restart_flag > 0 || at_check) {
                 const double g = m_norm();
                 if (tid == 0) {
@@ -1202,7 +1233,7 @@ struct AdjArgs {
 constexpr int kAdjGlobalN = 5, kAdjGlobalM = 4;  // sol, w_old, w, w_new (+ Q v) per CTA in global memory
 constexpr int kAdjLanczos = 3;                   // v_old, v, v_new (n and m parts)
 
-__global__ void __launch_bounds__(kBT, 1024 / kBT) k_batch_adjoint(const AdjArgs B)
+__global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_adjoint(const AdjArgs B)
 {
     extern __shared__ __align__(16) double dyn_smem[];
     __shared__ double s_red[kBW][8];
@@ -1450,6 +1481,37 @@ static HPRQPStatus balloc(HPRQPBatch *b, T **p, size_t count)
     return HPRQP_STATUS_OK;
 }
 
+// Several device arrays carved out of one allocation (256-byte aligned
+// slices): a batch's arrays are created together and freed together, and
+// one cudaMalloc instead of forty keeps small batches (and solve_gpu of a
+// small model) cheap to set up.
+class Carver {
+public:
+    template <class T>
+    Carver &add(T **p, size_t count)
+    {
+        req_.push_back({(void **)p, std::max<size_t>(count, 1) * sizeof(T)});
+        return *this;
+    }
+    HPRQPStatus commit(HPRQPBatch *b)
+    {
+        size_t total = 0;
+        for (auto &r : req_) total += (r.second + 255) & ~size_t(255);
+        char *base = nullptr;
+        HPRQPStatus st = balloc(b, &base, total);
+        if (st != HPRQP_STATUS_OK) return st;
+        size_t off = 0;
+        for (auto &r : req_) {
+            *r.first = base + off;
+            off += (r.second + 255) & ~size_t(255);
+        }
+        return HPRQP_STATUS_OK;
+    }
+
+private:
+    std::vector<std::pair<void **, size_t>> req_;
+};
+
 static void batch_free(HPRQPBatch *b)
 {
     for (void *p : b->allocs) cudaFree(p);
@@ -1464,19 +1526,21 @@ static void batch_free(HPRQPBatch *b)
 
 // The per-instance SpMV autotuner: the lane-group width of cta_spmv for one
 // matrix, from its row lengths.  For every width g = 1, 2, ..., 32 it walks
-// the rows exactly as cta_spmv does (kBW contiguous warp ranges, chunks of 32
-// rows, passes of 32/g rows, rounds of g*kU entries, the longest row of a
-// pass setting its rounds) and charges each warp
+// the rows exactly as cta_spmv does (kBW contiguous warp ranges, chunks of
+// 32 rows, passes of 32/g rows, rounds of one aligned quad per lane, the row
+// with the most quads in a pass setting its rounds) and charges each warp
 //     kChunkCost per chunk + per pass (kPassCost + log2(g) kShuffleCost
 //     + rounds * kRoundCost);
 // the warp with the largest charge sets the product's time, and the width
 // with the smallest such time wins (ties: the wider group, whose loads are
-// better coalesced).  The charges are in units of about 50 SM cycles:
-// a round is a global load, a dependent gather and kU dependent FMAs, a
-// shuffle step is one shuffle of a double, a pass re-reads two row pointers
-// from registers and moves the row sums.  The weights come from timing
-// each forced width over the 4096-QP batch recipe (hprqp_batch_set_spmv_lanes).
-constexpr double kRoundCost = 12.0, kShuffleCost = 0.6, kPassCost = 1.5, kChunkCost = 4.0;
+// better coalesced).  A round is a 16-byte index load and two 16-byte value
+// loads, four dependent gathers and FMAs; a shuffle step is one shuffle of a
+// double; a pass moves two row pointers and writes the row sums; a chunk
+// reads 33 row pointers and runs the caller's epilogue on its rows.  The
+// weights are least-squares fits to the per-instance times of the 4096-QP
+// batch recipe solved with each width forced (hprqp_batch_set_spmv_lanes),
+// in arbitrary units: a pass costs half a round and a chunk four rounds.
+constexpr double kRoundCost = 23.1, kShuffleCost = 0.59, kPassCost = 11.6, kChunkCost = 94.3;
 
 static double lane_group_cost(const size_t *rp, int nrow, int lg)
 {
@@ -1490,10 +1554,10 @@ static double lane_group_cost(const size_t *rp, int nrow, int lg)
             const int nr = std::min(32, w1 - c0);
             cost += kChunkCost;
             for (int p0 = 0; p0 < nr; p0 += rpp) {
-                size_t longest = 0;
+                size_t most = 0;
                 for (int r = c0 + p0; r < std::min(c0 + p0 + rpp, c0 + nr); ++r)
-                    longest = std::max(longest, rp[r + 1] - rp[r]);
-                const size_t rounds = (longest + (size_t)(g * kU) - 1) / (size_t)(g * kU);
+                    if (rp[r + 1] > rp[r]) most = std::max(most, ((rp[r + 1] + 3) >> 2) - (rp[r] >> 2));
+                const size_t rounds = (most + (size_t)g - 1) / (size_t)g;
                 cost += kPassCost + lg * kShuffleCost + (double)rounds * kRoundCost;
             }
         }
@@ -1557,7 +1621,7 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
                                      const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c,
                                      const double *AL, const double *AU, const double *l, const double *u,
                                      const double *obj_constants, int device_number, bool keep_caller_csr,
-                                     HPRQPBatch **out)
+                                     HPRQPBatch **out, bool abortable = true)
 {
     using namespace hpr;
     if (!out || !var_offsets || !row_offsets || !Q || !A || !c || !l || !u || K == 0)
@@ -1664,8 +1728,10 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         I.n = (int)M.Q.ncol;
         I.m = (int)M.A.nrow;
         I.obj_constant = M.obj_constant;
-        qnz += M.Q.nnz;
-        anz += M.A.nnz;
+        // every instance's entries start on a 4-entry (16-byte) boundary, so
+        // cta_spmv can read aligned quads of indices and values
+        qnz += (M.Q.nnz + 3) & ~size_t(3);
+        anz += (M.A.nnz + 3) & ~size_t(3);
         qrp += M.Q.nrow + 1;
         arp += M.A.nrow + 1;
         atrp += M.AT.nrow + 1;
@@ -1681,13 +1747,22 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     }
     b->total_n = nv;
     b->total_m = nr;
-    HostVec<int> h_qrp(qrp), h_arp(arp), h_atrp(atrp), h_qci(std::max<size_t>(qnz, 1)),
-        h_aci(std::max<size_t>(anz, 1)), h_atci(std::max<size_t>(anz, 1));
-    HostVec<double> h_qv(std::max<size_t>(qnz, 1)), h_av(std::max<size_t>(anz, 1)), h_atv(std::max<size_t>(anz, 1)),
+    // + 4: the last quad of the last instance stays inside the arrays
+    qnz += 4;
+    anz += 4;
+    HostVec<int> h_qrp(qrp), h_arp(arp), h_atrp(atrp), h_qci(qnz), h_aci(anz), h_atci(anz);
+    HostVec<double> h_qv(qnz), h_av(anz), h_atv(anz),
         h_c(std::max<size_t>(nv, 1)), h_l(std::max<size_t>(nv, 1)), h_u(std::max<size_t>(nv, 1)),
         h_AL(std::max<size_t>(nr, 1)), h_AU(std::max<size_t>(nr, 1));
-    h_qci[0] = h_aci[0] = h_atci[0] = 0;
-    h_qv[0] = h_av[0] = h_atv[0] = h_c[0] = h_l[0] = h_u[0] = h_AL[0] = h_AU[0] = 0.0;
+    h_c[0] = h_l[0] = h_u[0] = h_AL[0] = h_AU[0] = 0.0;
+    for (size_t e = qnz - 4; e < qnz; ++e) {
+        h_qci[e] = 0;
+        h_qv[e] = 0.0;
+    }
+    for (size_t e = anz - 4; e < anz; ++e) {
+        h_aci[e] = h_atci[e] = 0;
+        h_av[e] = h_atv[e] = 0.0;
+    }
     b->tuned_lg.assign(3 * K, 0);
     auto pack_worker = [&](unsigned tix) {
     for (size_t k = tix; k < K; k += nth) {
@@ -1703,11 +1778,19 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
             h_qci[I.q_nz + e] = (int)M.Q.col_ind[e];
             h_qv[I.q_nz + e] = M.Q.values[e];
         }
+        for (size_t e = M.Q.nnz; e < ((M.Q.nnz + 3) & ~size_t(3)); ++e) {  // alignment padding
+            h_qci[I.q_nz + e] = 0;
+            h_qv[I.q_nz + e] = 0.0;
+        }
         for (size_t e = 0; e < M.A.nnz; ++e) {
             h_aci[I.a_nz + e] = (int)M.A.col_ind[e];
             h_av[I.a_nz + e] = M.A.values[e];
             h_atci[I.at_nz + e] = (int)M.AT.col_ind[e];
             h_atv[I.at_nz + e] = M.AT.values[e];
+        }
+        for (size_t e = M.A.nnz; e < ((M.A.nnz + 3) & ~size_t(3)); ++e) {
+            h_aci[I.a_nz + e] = h_atci[I.at_nz + e] = 0;
+            h_av[I.a_nz + e] = h_atv[I.at_nz + e] = 0.0;
         }
         memcpy(&h_c[I.var], M.c, M.Q.ncol * sizeof(double));
         memcpy(&h_l[I.var], M.l, M.Q.ncol * sizeof(double));
@@ -1743,24 +1826,17 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     double *d_qv0, *d_av0, *d_atv0, *d_c, *d_l, *d_u, *d_AL, *d_AU;
     BInst *d_inst;
     int *d_order, *d_counter;
-    if ((st = balloc(b, &d_qrp, qrp)) || (st = balloc(b, &d_arp, arp)) || (st = balloc(b, &d_atrp, atrp)) ||
-        (st = balloc(b, &d_qci, h_qci.size())) || (st = balloc(b, &d_aci, h_aci.size())) ||
-        (st = balloc(b, &d_atci, h_atci.size())) || (st = balloc(b, &d_qv0, h_qv.size())) ||
-        (st = balloc(b, &d_av0, h_av.size())) || (st = balloc(b, &d_atv0, h_atv.size())) ||
-        (st = balloc(b, &G.q_v, h_qv.size())) || (st = balloc(b, &G.a_v, h_av.size())) ||
-        (st = balloc(b, &G.at_v, h_atv.size())) || (st = balloc(b, &d_c, h_c.size())) ||
-        (st = balloc(b, &d_l, h_l.size())) || (st = balloc(b, &d_u, h_u.size())) ||
-        (st = balloc(b, &d_AL, h_AL.size())) || (st = balloc(b, &d_AU, h_AU.size())) ||
-        (st = balloc(b, &d_inst, K)) || (st = balloc(b, &d_order, K)) || (st = balloc(b, &d_counter, 1)) ||
-        (st = balloc(b, &G.x, h_c.size())) || (st = balloc(b, &G.z, h_c.size())) || (st = balloc(b, &G.w, h_c.size())) ||
-        (st = balloc(b, &G.y, h_AL.size())) || (st = balloc(b, &G.status, K)) || (st = balloc(b, &G.iters, K)) ||
-        (st = balloc(b, &G.pobj, K)) || (st = balloc(b, &G.resid, K)) || (st = balloc(b, &G.gap, K)) ||
-        (st = balloc(b, &G.restarts, K)) || (st = balloc(b, &G.sigma_out, K)) ||
-        (st = balloc(b, &G.seconds_out, K)) ||
-        (st = balloc(b, &G.active_x, h_c.size())) ||
-        (st = balloc(b, &G.active_r, h_AL.size())) || (st = balloc(b, &G.col_norm_out, h_c.size())) ||
-        (st = balloc(b, &G.row_norm_out, h_AL.size())))
-        return fail(st);
+    Carver cv;
+    cv.add(&d_qrp, qrp).add(&d_arp, arp).add(&d_atrp, atrp).add(&d_qci, h_qci.size()).add(&d_aci, h_aci.size());
+    cv.add(&d_atci, h_atci.size()).add(&d_qv0, h_qv.size()).add(&d_av0, h_av.size()).add(&d_atv0, h_atv.size());
+    cv.add(&G.q_v, h_qv.size()).add(&G.a_v, h_av.size()).add(&G.at_v, h_atv.size());
+    cv.add(&d_c, h_c.size()).add(&d_l, h_l.size()).add(&d_u, h_u.size()).add(&d_AL, h_AL.size()).add(&d_AU, h_AU.size());
+    cv.add(&d_inst, K).add(&d_order, K).add(&d_counter, 1);
+    cv.add(&G.x, h_c.size()).add(&G.z, h_c.size()).add(&G.w, h_c.size()).add(&G.y, h_AL.size());
+    cv.add(&G.status, K).add(&G.iters, K).add(&G.pobj, K).add(&G.resid, K).add(&G.gap, K).add(&G.restarts, K);
+    cv.add(&G.sigma_out, K).add(&G.seconds_out, K).add(&G.active_x, h_c.size()).add(&G.active_r, h_AL.size());
+    cv.add(&G.col_norm_out, h_c.size()).add(&G.row_norm_out, h_AL.size()).add(&b->d_t0, 1);
+    if ((st = cv.commit(b))) return fail(st);
     // largest instances first
     std::vector<int> order(K);
     std::iota(order.begin(), order.end(), 0);
@@ -1781,10 +1857,14 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         !up(d_AU, h_AU.data(), h_AU.size() * 8) || !up(d_inst, b->inst.data(), K * sizeof(BInst)) ||
         !up(d_order, order.data(), K * sizeof(int)) || cudaStreamSynchronize(b->stream) != cudaSuccess)
         return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
-    if (cudaHostAlloc((void **)&b->h_abort, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
-        cudaHostGetDevicePointer((void **)&b->d_abort, b->h_abort, 0) != cudaSuccess)
-        return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
-    __atomic_store_n(b->h_abort, 0, __ATOMIC_SEQ_CST);
+    // the abort flag (host-mapped memory) exists only for batches a caller
+    // holds a handle to: the one-call forms cannot be asked to stop
+    if (abortable) {
+        if (cudaHostAlloc((void **)&b->h_abort, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostGetDevicePointer((void **)&b->d_abort, b->h_abort, 0) != cudaSuccess)
+            return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
+        __atomic_store_n(b->h_abort, 0, __ATOMIC_SEQ_CST);
+    }
     G.abort_flag = b->d_abort;
     G.inst = d_inst;
     b->d_inst = d_inst;
@@ -1829,7 +1909,7 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     B_CK(cudaSetDevice(b->device));
     BatchArgs &G = b->args;
     const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
-    const size_t vec_bytes = (4 * na + 2 * ma) * sizeof(double);
+    const size_t vec_bytes = (4 * na + 2 * ma) * sizeof(double);  // the gathered vectors
     G.vec_smem = HPR_BATCH_VEC_SMEM && vec_bytes <= kSmemLimit;
     const size_t smem = G.vec_smem ? vec_bytes : 0;
     B_CK(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1851,10 +1931,6 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     G.check_iter = (int)p->check_iter;
     G.print_frequency = p->print_frequency;
     G.use_scaling = p->use_scaling;
-    if (!b->d_t0) {
-        HPRQPStatus st = balloc(b, &b->d_t0, 1);
-        if (st) return st;
-    }
     unsigned long long *d_t0 = b->d_t0;
     B_CK(cudaMemsetAsync(G.counter, 0, sizeof(int), b->stream));
     k_batch_clock<<<1, 1, 0, b->stream>>>(d_t0);
@@ -1891,7 +1967,7 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     b->last_ms = ms;
     b->solved = true;
     // an abort request ends with the solve it stopped
-    __atomic_store_n(b->h_abort, 0, __ATOMIC_SEQ_CST);
+    if (b->h_abort) __atomic_store_n(b->h_abort, 0, __ATOMIC_SEQ_CST);
     if (d_phase) {
         std::vector<unsigned long long> h((size_t)grid * 8);
         B_CK(cudaMemcpy(h.data(), d_phase, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -2246,7 +2322,7 @@ HPRQPStatus hprqp_solve_batch(size_t K, const size_t *var_offsets, const size_t 
     const double t0 = now();
     HPRQPBatch *b = nullptr;
     HPRQPStatus st = batch_create_impl(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants,
-                                       params->device_number, false, &b);
+                                       params->device_number, false, &b, false);
     if (st != HPRQP_STATUS_OK) return st;
     const double t1 = now();
     st = hprqp_batch_solve(b, params);
@@ -2300,15 +2376,18 @@ HPRQPStatus solve_single_cta(const HPRQPModel *model, const HPRQPParams *params,
     HPRQPBatch *b = nullptr;
     // the model is already preprocessed; the builder's rules leave it unchanged
     HPRQPStatus st = batch_create_impl(1, var_off, row_off, &model->Q, &model->A, model->c, model->AL, model->AU,
-                                       model->l, model->u, &model->obj_constant, params->device_number, false, &b);
+                                       model->l, model->u, &model->obj_constant, params->device_number, false, &b,
+                                       false);
     if (st != HPRQP_STATUS_OK) return st;
     BatchArgs &G = b->args;
     long long *d_i4 = nullptr, *d_i6 = nullptr;
     double *d_t = nullptr, *d_log = nullptr;
     int *d_logn = nullptr;
     const size_t cap = log_records ? std::min(log_cap, log_records_needed(params)) : 0;
-    if ((st = balloc(b, &d_i4, 1)) || (st = balloc(b, &d_i6, 1)) || (st = balloc(b, &d_t, 3)) ||
-        (st = balloc(b, &d_logn, 1)) || (cap && (st = balloc(b, &d_log, cap * kLogFields)))) {
+    Carver cv;
+    cv.add(&d_i4, 1).add(&d_i6, 1).add(&d_t, 3).add(&d_logn, 1);
+    if (cap) cv.add(&d_log, cap * kLogFields);
+    if ((st = cv.commit(b))) {
         hprqp_batch_destroy(b);
         return st;
     }
