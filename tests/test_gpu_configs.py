@@ -13,6 +13,8 @@ the original model.
   nnz(Q)=3.2e7) for fixed iteration budgets of 200 and 1000 iterations:
   both solvers stop at MAX_ITER; their KKT residuals and objectives agree
   within the drift of two FP64 trajectories whose SpMVs round differently.
+  (The full-size recipe does not reach 1e-6 within minutes on either
+  solver: after 90 s this engine is at KKT 1.4e-2, iteration 188,100.)
 """
 from __future__ import annotations
 
@@ -73,7 +75,8 @@ def test_large_qp_full_size_fixed_budget_matches_reference_gpu(engine_lib, budge
     r = _ours(engine_lib, inst, 1e-8, max_iter=budget)
     assert r.status_code == ref["status"] == engine_lib.STATUS_MAX_ITER
     assert int(r.iter) == ref["iter"] == budget
-    # same trajectory up to rounding drift: the KKT residuals within 5% of
-    # each other and the objectives within 1e-3 relative after the budget
-    assert abs(r.residual - ref["residuals"]) <= 0.05 * ref["residuals"], (r.residual, ref["residuals"])
-    assert _rel(r.objective, ref["primal_obj"]) <= 1e-3, (r.objective, ref["primal_obj"])
+    # same trajectory up to rounding drift (measured on a B200: KKT residuals
+    # equal to 1e-15 relative after 200 iterations and 1e-9 after 1000,
+    # objectives to 1e-14): KKT within 1e-6 and objectives within 1e-9
+    assert abs(r.residual - ref["residuals"]) <= 1e-6 * ref["residuals"], (r.residual, ref["residuals"])
+    assert _rel(r.objective, ref["primal_obj"]) <= 1e-9, (r.objective, ref["primal_obj"])
