@@ -358,7 +358,9 @@ def large_qp_leg(peak_gbs: float, iters: int = 3000, minres_iters: int = 2000, s
     reach 1e-8 within minutes, neither here nor with the reference's GPU
     build): HPR iterations/s of the solve loop and the HBM roofline of its
     algorithmic bytes (B_iter per iteration); then the single-instance
-    adjoint (hprqp_diff.h) on that iterate."""
+    adjoint (hprqp_diff.h) on that unconverged iterate for a fixed MINRES
+    budget (time per MINRES iteration; large_backward_leg has the converged
+    case)."""
     import hprqp
     from hprqp import instances
 
@@ -383,6 +385,34 @@ def large_qp_leg(peak_gbs: float, iters: int = 3000, minres_iters: int = 2000, s
         out["backward"] = {"minres_iters": g["minres_iters"], "relres": g["minres_relres"],
                            "seconds": round(g["backward_seconds"], 3),
                            "ms_per_minres_iter": round(1e3 * g["backward_seconds"] / max(g["minres_iters"], 1), 4)}
+    return out
+
+
+def large_backward_leg(scale: float = 1.0, tol: float = 1e-10, max_minres: int = 50000):
+    """The single large backward at the large QP's sizes (n=1e6, m=5e5,
+    nnz(A)=1e7, nnz(Q)~3.2e7) on the plain recipe, whose forward solve reaches
+    1e-8 (the power-law recipe does not within minutes): forward
+    solve_for_backward to 1e-8, then hprqp_backward with MINRES to a relative
+    residual of 1e-10; times of both calls and their ratio."""
+    import hprqp
+    from hprqp import instances
+
+    inst = instances.config1_sized_plain(scale=scale)
+    model = hprqp.build_from_instance(inst)
+    params = hprqp.Parameters(verbose=False, stoptol=1e-8, time_limit=300.0)
+    t0 = time.perf_counter()
+    r, state = hprqp.solve_for_backward(model, params)
+    fwd = time.perf_counter() - t0
+    out = {"workload": f"plain recipe at n={inst.n} m={inst.m} nnz(A)={inst.A.nnz} nnz(Q)={inst.Q.nnz}, stoptol 1e-8",
+           "status": r.status, "iterations": int(r.iter), "kkt": float(r.residual), "forward_call_s": round(fwd, 3),
+           "forward_loop_s": round(r.time, 3)}
+    if state is not None:
+        g = state.backward(np.random.default_rng(1).standard_normal(inst.n), tol=tol, max_iter=max_minres)
+        state.close()
+        out.update(minres_iters=int(g["minres_iters"]), minres_relres=float(g["minres_relres"]),
+                   backward_s=round(g["backward_seconds"], 3),
+                   ms_per_minres_iter=round(1e3 * g["backward_seconds"] / max(g["minres_iters"], 1), 4),
+                   backward_over_forward=round(g["backward_seconds"] / fwd, 3))
     return out
 
 
@@ -544,7 +574,8 @@ def main():
     ap.add_argument("--no-plain-large", action="store_true")
     ap.add_argument("--no-warm", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
-    ap.add_argument("--only", choices=["spmv", "batch", "adjoint", "large", "portfolio", "warm", "reference_gpu"],
+    ap.add_argument("--only", choices=["spmv", "batch", "adjoint", "large", "large_backward", "portfolio", "warm",
+                                       "reference_gpu"],
                     default=None,
                     help="sub-runs: only the large-QP SpMV leg, the batched solve, the adjoint, the large-QP "
                          "plain solve, the portfolio plain solve, the warm-start re-solve or the reference GPU "
@@ -611,6 +642,9 @@ def main():
     if args.only == "large":
         print(json.dumps({"large_qp": large_qp_leg(peak, args.large_iters, args.minres_iters, args.scale)}),
               flush=True)
+        return
+    if args.only == "large_backward":
+        print(json.dumps({"large_backward": large_backward_leg(args.scale)}), flush=True)
         return
     if args.only == "portfolio":
         print(json.dumps({"portfolio": portfolio_leg()}), flush=True)
@@ -719,6 +753,7 @@ def main():
             line["warm_start"] = warm_start_leg(packed, res, local_rank)
         if not args.no_plain_large:
             line["large_qp"] = large_qp_leg(peak)
+            line["large_backward"] = large_backward_leg()
             line["portfolio"] = portfolio_leg()
         if not args.no_reference_gpu:
             line["reference_gpu"] = reference_gpu_leg(local_rank)

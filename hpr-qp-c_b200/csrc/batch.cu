@@ -41,26 +41,25 @@
 
 namespace hpr {
 
-// 1024 threads, one CTA (one instance) per SM.  Measured on the 4096-QP
-// batch with the quad-load SpMV: 865 solves/s, against 779 for 512 threads
-// x 2 CTAs per SM; 148 instances in flight keep more of their matrices in
-// L2 than 296, and each instance gets twice the warps.
-#ifndef HPR_BATCH_THREADS
-#define HPR_BATCH_THREADS 1024
-#endif
+// Two CTA shapes, chosen per batch: 1024 threads and one CTA (one instance)
+// per SM -- measured on the 4096-QP batch with the quad-load SpMV: 851
+// solves/s, against 705 for 512 threads x 2 CTAs per SM (148 instances in
+// flight keep more of their matrices in L2 than 296, and each instance gets
+// twice the warps) -- except for batches of one to two instances per SM,
+// which run in one wave of 512-thread CTAs (256 QPs of n = 500: forward
+// 118 ms against 126 ms, adjoint 15.7 ms against 21.1 ms).
 #ifndef HPR_BATCH_LD
 #define HPR_BATCH_LD __ldg  // instance matrices are re-read every iteration: keep them in L2
 #endif
 #ifndef HPR_BATCH_VEC_SMEM
 #define HPR_BATCH_VEC_SMEM 1
 #endif
-constexpr int kBT = HPR_BATCH_THREADS;  // threads per CTA of the batch kernel
-constexpr int kBW = kBT / 32;
-constexpr int kCtasPerSm = kBT >= 1024 ? 1 : 1024 / kBT;
-// dynamic shared memory per CTA: the gathered vectors and the SpMV row-sum
-// arrays move to shared memory when they fit (every instance of n, m <=
-// 2000 at one CTA per SM), else they stay in global memory (L1-cached)
-constexpr size_t kSmemLimit = kCtasPerSm == 1 ? 200 * 1024 : 110 * 1024;
+constexpr int kBigCta = 1024, kSmallCta = 512;
+constexpr int ctas_per_sm(int bt) { return bt >= 1024 ? 1 : 1024 / bt; }
+// dynamic shared memory per CTA: the gathered vectors move to shared memory
+// when they fit (every instance of n, m <= 2000), else they stay in global
+// memory (L1-cached)
+constexpr size_t smem_limit(int bt) { return ctas_per_sm(bt) == 1 ? 200 * 1024 : 110 * 1024; }
 
 struct BInst {
     long long q_nz, a_nz, at_nz;  // first entry of the instance's matrices
@@ -169,7 +168,7 @@ __device__ __forceinline__ double clampd(double v, double lo, double hi)
 }
 
 // fold per-thread values over the CTA; every thread gets the results
-template <int N>
+template <int N, int kBW>
 __device__ __forceinline__ void cta_allreduce(double (&v)[N], const int (&ops)[N], double (*s_red)[8],
                                               double *s_out)
 {
@@ -195,6 +194,7 @@ __device__ __forceinline__ void cta_allreduce(double (&v)[N], const int (&ops)[N
 // contiguous range per warp, balanced to within one row.  It depends on
 // nrow only, so products with Q and A' (both n rows) call their epilogues
 // for a row on the same thread.
+template <int kBW>
 __device__ __forceinline__ void warp_rows(int nrow, int warp, int &r0, int &r1)
 {
     const int per = (nrow + kBW - 1) / kBW;
@@ -215,16 +215,17 @@ __device__ __forceinline__ void warp_rows(int nrow, int warp, int &r0, int &r1)
 // into its own sum in entry order.  The group folds its g sums with an
 // xor-shuffle tree and the row's value moves to the lane that owns the row.
 // The summation order depends on g only.
-template <class F>
+template <int BT, class F>
 __device__ __forceinline__ void cta_spmv(const LCsr &M, const double *x, F &&f)
 {
+    constexpr int kBW = BT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lg = M.lg, g = 1 << lg, sh = 5 - lg, rpp = 32 >> lg;
     const int gl = lane & (g - 1), grp = lane >> lg;
     const int4 *ci4 = reinterpret_cast<const int4 *>(M.ci);
     const double2 *v2 = reinterpret_cast<const double2 *>(M.v);
     int w0, w1;
-    warp_rows(M.nrow, warp, w0, w1);
+    warp_rows<kBW>(M.nrow, warp, w0, w1);
     for (int c0 = w0; c0 < w1; c0 += 32) {
         const int nr = min(32, w1 - c0);
         const int my_b = lane < nr ? M.rp[c0 + lane] : 0;
@@ -241,18 +242,13 @@ __device__ __forceinline__ void cta_spmv(const LCsr &M, const double *x, F &&f)
                 for (int q = (b >> 2) + gl; q < q1; q += g) {
                     const int4 c = HPR_BATCH_LD(ci4 + q);
                     const double2 va = HPR_BATCH_LD(v2 + 2 * q), vb = HPR_BATCH_LD(v2 + 2 * q + 1);
+                    // every entry masked (a branch for the quads inside the
+                    // row measured 10 % slower: the lanes of a group diverge)
                     const int k0 = 4 * q;
-                    if (k0 >= b && k0 + 4 <= e) {  // a quad inside the row
-                        s = fma(va.x, x[c.x], s);
-                        s = fma(va.y, x[c.y], s);
-                        s = fma(vb.x, x[c.z], s);
-                        s = fma(vb.y, x[c.w], s);
-                    } else {  // the first or last quad of the row
-                        if (k0 >= b && k0 < e) s = fma(va.x, x[c.x], s);
-                        if (k0 + 1 >= b && k0 + 1 < e) s = fma(va.y, x[c.y], s);
-                        if (k0 + 2 >= b && k0 + 2 < e) s = fma(vb.x, x[c.z], s);
-                        if (k0 + 3 >= b && k0 + 3 < e) s = fma(vb.y, x[c.w], s);
-                    }
+                    if (k0 >= b && k0 < e) s = fma(va.x, x[c.x], s);
+                    if (k0 + 1 >= b && k0 + 1 < e) s = fma(va.y, x[c.y], s);
+                    if (k0 + 2 >= b && k0 + 2 < e) s = fma(vb.x, x[c.z], s);
+                    if (k0 + 3 >= b && k0 + 3 < e) s = fma(vb.y, x[c.w], s);
                 }
             }
             for (int o = g >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -317,6 +313,7 @@ static __device__ Vecs carve(double *base, int nmax, int mmax, double *smem_pool
     return V;
 }
 
+template <int kBW>
 __device__ __forceinline__ void scale_rows(const LCsr &M, double *vals, const double *rs, const double *cs)
 {
     // v *= 1/rs[row]; v /= cs[col]  (reference scale.cu:113-150 roundings)
@@ -343,9 +340,11 @@ __device__ __forceinline__ double row_abs(const LCsr &M, int r, bool sum)
 }
 
 // Power iteration (reference src/gpu/eigs.cu:185-383), CTA-wide.
+template <int BT>
 static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q, bool is_a, int len, double *z,
                             double *q, double *tmp, double (*s_red)[8], double *s_out)
 {
+    constexpr int kBT = BT, kBW = BT / 32;
     if (len == 0) return 0.0;
     const int tid = threadIdx.x;
     for (int i = tid; i < len; i += kBT) z[i] = 1.0 + ((double)i + 1.0) / ((double)len + 1.0);
@@ -353,7 +352,7 @@ static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q,
     const int ops1[1] = {kSum};
     for (int i = tid; i < len; i += kBT) v1[0] += z[i] * z[i];
     __syncthreads();
-    cta_allreduce<1>(v1, ops1, s_red, s_out);
+    cta_allreduce<1, kBW>(v1, ops1, s_red, s_out);
     double zz = v1[0], lambda = 1.0;
     for (int it = 0; it < 5000; ++it) {
         const double qn = sqrt(zz);
@@ -367,22 +366,22 @@ static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q,
         double v2[2] = {0.0, 0.0};
         const int ops2[2] = {kSum, kSum};
         if (is_a) {
-            cta_spmv(AT, q, [&](int r, double s) { tmp[r] = s; });
+            cta_spmv<kBT>(AT, q, [&](int r, double s) { tmp[r] = s; });
             __syncthreads();
-            cta_spmv(A, tmp, [&](int r, double s) {
+            cta_spmv<kBT>(A, tmp, [&](int r, double s) {
                 z[r] = s;
                 v2[0] += q[r] * s;
                 v2[1] += s * s;
             });
         } else {
-            cta_spmv(Q, q, [&](int r, double s) {
+            cta_spmv<kBT>(Q, q, [&](int r, double s) {
                 z[r] = s;
                 v2[0] += q[r] * s;
                 v2[1] += s * s;
             });
         }
         __syncthreads();
-        cta_allreduce<2>(v2, ops2, s_red, s_out);
+        cta_allreduce<2, kBW>(v2, ops2, s_red, s_out);
         lambda = v2[0];
         zz = v2[1];
         const double zn = sqrt(zz);
@@ -393,7 +392,7 @@ static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q,
             v3[0] += r * r;
         }
         __syncthreads();
-        cta_allreduce<1>(v3, ops1, s_red, s_out);
+        cta_allreduce<1, kBW>(v3, ops1, s_red, s_out);
         if (sqrt(v3[0]) / (zn + fabs(lambda) + 1e-16) < 1e-4) break;
     }
     return lambda < 0.0 ? 0.0 : lambda;
@@ -429,16 +428,17 @@ static __device__ __forceinline__ bool on_print_grid(long long iter)
     return iter % (long long)adaptive_step_d(iter) == 0;
 }
 
-__global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs B)
+template <int BT>
+__global__ void __launch_bounds__(BT, ctas_per_sm(BT)) k_batch_solve(const BatchArgs B)
 {
+    constexpr int kBT = BT, kBW = BT / 32;
     extern __shared__ __align__(16) double dyn_smem[];
     __shared__ CtaState S;
     __shared__ double s_red[kBW][8];
     __shared__ double s_out[8];
     __shared__ int s_inst, s_skip;
     const int tid = threadIdx.x;
-    Vecs V = carve(B.ws + (size_t)blockIdx.x * B.ws_stride, B.nmax, B.mmax,
-                   B.vec_smem ? dyn_smem : nullptr);
+    Vecs V = carve(B.ws + (size_t)blockIdx.x * B.ws_stride, B.nmax, B.mmax, B.vec_smem ? dyn_smem : nullptr);
 
     for (;;) {
         if (tid == 0) {
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                 v[0] = fmax(v[0], lo > hi ? lo : hi);
             }
             for (int i = tid; i < n; i += kBT) v[1] = fmax(v[1], fabs(V.c[i]));
-            cta_allreduce<2>(v, ops, s_red, s_out);
+            cta_allreduce<2, kBW>(v, ops, s_red, s_out);
             if (tid == 0) {
                 S.norm_b_org = v[0];
                 S.norm_c_org = v[1];
@@ -541,10 +541,10 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                     if (lane == 0) V.fac_r[r] = a > 0.0 ? sqrt(a) : 1.0;
                 }
                 __syncthreads();
-                scale_rows(Q, qv, V.fac_c, V.fac_c);
+                scale_rows<kBW>(Q, qv, V.fac_c, V.fac_c);
                 if (m > 0) {
-                    scale_rows(A, av, V.fac_r, V.fac_c);
-                    scale_rows(AT, atv, V.fac_c, V.fac_r);
+                    scale_rows<kBW>(A, av, V.fac_r, V.fac_c);
+                    scale_rows<kBW>(AT, atv, V.fac_c, V.fac_r);
                 }
                 for (int i = tid; i < n; i += kBT) {
                     const double f = V.fac_c[i];
@@ -592,10 +592,10 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                 diagmax = fmax(diagmax, fabs(d));
             }
             v[3] = offmax;
-            cta_allreduce<4>(v, ops, s_red, s_out);
+            cta_allreduce<4, kBW>(v, ops, s_red, s_out);
             double v2[1] = {diagmax};
             const int ops2[1] = {kMax};
-            cta_allreduce<1>(v2, ops2, s_red, s_out);
+            cta_allreduce<1, kBW>(v2, ops2, s_red, s_out);
             if (tid == 0) {
                 const double nb = sqrt(v[0]), nc = sqrt(v[1]);
                 S.sigma = (nb > 1e-16 && nc > 1e-16 && nb < 1e16 && nc < 1e16) ? nb / nc : 1.0;
@@ -611,11 +611,11 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
         }
         PHASE_ADD(1);
         if (!S.q_is_diag) {
-            const double lq = (q_nnz > 0) ? cta_power(A, AT, Q, false, n, V.pn, V.tempv, V.Qx, s_red, s_out) : 0.0;
+            const double lq = (q_nnz > 0) ? cta_power<kBT>(A, AT, Q, false, n, V.pn, V.tempv, V.Qx, s_red, s_out) : 0.0;
             if (tid == 0) S.lQ = lq * 1.05;
         }
         {
-            const double la = m > 0 ? cta_power(A, AT, Q, true, m, V.pz, V.pq, V.pn, s_red, s_out) : 0.0;
+            const double la = m > 0 ? cta_power<kBT>(A, AT, Q, true, m, V.pz, V.pq, V.pn, s_red, s_out) : 0.0;
             if (tid == 0) S.lA = la * 1.05;
         }
         __syncthreads();
@@ -650,8 +650,8 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
             // the products the step carries with the iterates: A'y, and Q w
             // on the noC path (reference iteration.cu:831-920)
             if (m > 0)
-                cta_spmv(AT, V.y, [&](int i, double s) { V.ATy[i] = V.ATy_bar[i] = V.last_ATy[i] = s; });
-            if (S.noC) cta_spmv(Q, V.w, [&](int i, double s) { V.Qw[i] = V.Qw_bar[i] = V.last_Qw[i] = s; });
+                cta_spmv<kBT>(AT, V.y, [&](int i, double s) { V.ATy[i] = V.ATy_bar[i] = V.last_ATy[i] = s; });
+            if (S.noC) cta_spmv<kBT>(Q, V.w, [&](int i, double s) { V.Qw[i] = V.Qw_bar[i] = V.last_Qw[i] = s; });
         }
         if (tid == 0) {
             S.restart_flag = 0;
@@ -667,13 +667,13 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
 
         // ---- residuals (reference residuals.cu:81-183) ----------------------
         auto residuals = [&](long long iter) {
-            if (m > 0) cta_spmv(AT, V.y_bar, [&](int r, double s) { V.ATdy[r] = s; });
+            if (m > 0) cta_spmv<kBT>(AT, V.y_bar, [&](int r, double s) { V.ATdy[r] = s; });
             else
                 for (int i = tid; i < n; i += kBT) V.ATdy[i] = 0.0;
             double a[3] = {0.0, 0.0, 0.0};
             const int opa[3] = {kMax, kMax, kSum};
             if (m > 0)
-                cta_spmv(A, V.x_bar, [&](int r, double ax) {
+                cta_spmv<kBT>(A, V.x_bar, [&](int r, double ax) {
                     const double proj = clampd(ax, V.AL[r], V.AU[r]);
                     const double sf = V.row_norm[r];
                     V.Ax[r] = ax;
@@ -685,7 +685,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
             __syncthreads();
             double q[7] = {0, 0, 0, 0, 0, 0, 0};
             const int opq[7] = {kMax, kMax, kMax, kSum, kSum, kSum, kMax};
-            cta_spmv(Q, V.x_bar, [&](int r, double qx) {
+            cta_spmv<kBT>(Q, V.x_bar, [&](int r, double qx) {
                 const double sf = V.col_norm[r];
                 const double xb = V.x_bar[r], aty = V.ATdy[r];
                 V.Qx[r] = qx;
@@ -704,8 +704,8 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                     q[6] = fmax(q[6], fabs(vv * (1.0 / sf)));
                 }
             });
-            cta_allreduce<3>(a, opa, s_red, s_out);
-            cta_allreduce<7>(q, opq, s_red, s_out);
+            cta_allreduce<3, kBW>(a, opa, s_red, s_out);
+            cta_allreduce<7, kBW>(q, opq, s_red, s_out);
             if (tid == 0) {
                 S.pobj = (q[3] + 0.5 * q[4]) + S.obj_constant;
                 S.dobj = (-0.5 * q[4] + q[5] + a[2]) + S.obj_constant;
@@ -743,11 +743,11 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                     V.w_bar[i] = wb;
                     V.w[i] = h2 * (2.0 * wb - wi) + h1 * V.last_w[i];
                 };
-                if (m > 0) cta_spmv(AT, V.y, upd);
+                if (m > 0) cta_spmv<kBT>(AT, V.y, upd);
                 else
                     for (int i = tid; i < n; i += kBT) upd(i, 0.0);
                 __syncthreads();
-                cta_spmv(Q, V.w_bar, [&](int i, double qwb) {
+                cta_spmv<kBT>(Q, V.w_bar, [&](int i, double qwb) {
                     const double qw = V.Qw[i];
                     V.Qw_bar[i] = qwb;
                     V.Qw[i] = h2 * (2.0 * qwb - qw) + h1 * V.last_Qw[i];
@@ -755,7 +755,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                 });
                 __syncthreads();
             } else {
-                cta_spmv(Q, V.w, [&](int i, double qw) {
+                cta_spmv<kBT>(Q, V.w, [&](int i, double qw) {
                     const double xi = V.x[i], wi = V.w[i];
                     const double z_raw = xi + sigma * (-qw + V.ATy[i] - V.c[i]);
                     const double xb = clampd(z_raw, V.l[i], V.u[i]);
@@ -772,14 +772,14 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                 });
                 __syncthreads();
                 if (m > 0) {
-                    cta_spmv(Q, V.w_bar,
+                    cta_spmv<kBT>(Q, V.w_bar,
                              [&](int i, double qwb) { V.tempv[i] = V.x_hat[i] + sigma * (V.Qw[i] - qwb); });
                     __syncthreads();
                 }
             }
             if (m > 0) {
                 const double f1 = lA * sigma, f2 = 1.0 / f1;
-                cta_spmv(A, V.tempv, [&](int i, double ax) {
+                cta_spmv<kBT>(A, V.tempv, [&](int i, double ax) {
                     const double yi = V.y[i];
                     const double s_raw = ax - f1 * yi;
                     const double sp = clampd(s_raw, V.AL[i], V.AU[i]);
@@ -809,7 +809,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                     V.w[i] = h1 * V.last_w[i] + h2 * (2.0 * wbn - wi);
                     V.ATy[i] = h1 * V.last_ATy[i] + h2 * (2.0 * atyb - aty);
                 };
-                if (m > 0) cta_spmv(AT, V.y_bar, w2);
+                if (m > 0) cta_spmv<kBT>(AT, V.y_bar, w2);
                 else
                     for (int i = tid; i < n; i += kBT) w2(i, 0.0);
                 __syncthreads();
@@ -820,7 +820,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
         auto m_norm = [&]() -> double {
             double a[4] = {0, 0, 0, 0};
             const int ops4[4] = {kSum, kSum, kSum, kSum};
-            cta_spmv(Q, V.dw, [&](int i, double v) {
+            cta_spmv<kBT>(Q, V.dw, [&](int i, double v) {
                 V.dQw[i] = v;
                 const double dx = V.dx[i];
                 a[0] += dx * dx;
@@ -832,13 +832,13 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
             double b[2] = {0, 0}, c3[3] = {0, 0, 0};
             const int ops2[2] = {kSum, kSum}, ops3[3] = {kSum, kSum, kSum};
             if (m > 0) {
-                cta_spmv(AT, V.dy, [&](int i, double v) {
+                cta_spmv<kBT>(AT, V.dy, [&](int i, double v) {
                     V.ATdy[i] = v;
                     b[0] += v * V.dx[i];
                 });
                 for (int i = tid; i < m; i += kBT) b[1] += V.dy[i] * V.dy[i];
                 __syncthreads();
-                cta_spmv(Q, V.ATdy, [&](int i, double v) {
+                cta_spmv<kBT>(Q, V.ATdy, [&](int i, double v) {
                     V.QATdy[i] = v;
                     const double at = V.ATdy[i];
                     c3[0] += V.dQw[i] * at;
@@ -846,9 +846,9 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                     if (S.q_is_diag) c3[2] += (at * V.fact_M[i]) * v;
                 });
             }
-            cta_allreduce<4>(a, ops4, s_red, s_out);
-            cta_allreduce<2>(b, ops2, s_red, s_out);
-            cta_allreduce<3>(c3, ops3, s_red, s_out);
+            cta_allreduce<4, kBW>(a, ops4, s_red, s_out);
+            cta_allreduce<2, kBW>(b, ops2, s_red, s_out);
+            cta_allreduce<3, kBW>(c3, ops3, s_red, s_out);
             const double sigma = S.sigma, lA = S.lA, lQ = S.lQ;
             double m1 = 0.0, m3 = 0.0, m2 = (1.0 / sigma) * a[0];
             m2 -= 2.0 * a[1];
@@ -890,21 +890,21 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
             __syncthreads();
             double e3[3] = {0, 0, 0}, f1v[1] = {0};
             const int ops3[3] = {kSum, kSum, kSum}, ops1[1] = {kSum};
-            cta_spmv(Q, V.dw, [&](int i, double v) {
+            cta_spmv<kBT>(Q, V.dw, [&](int i, double v) {
                 V.dQw[i] = v;
                 if (m > 0) e3[0] += v * V.ATdy[i];
                 e3[1] += v * v;
                 e3[2] += V.dw[i] * v;
             });
             if (m > 0) {
-                cta_spmv(Q, V.ATdy, [&](int i, double v) {
+                cta_spmv<kBT>(Q, V.ATdy, [&](int i, double v) {
                     V.QATdy[i] = v;
                     f1v[0] += V.ATdy[i] * v;
                 });
             }
-            cta_allreduce<2>(d, ops2, s_red, s_out);
-            cta_allreduce<3>(e3, ops3, s_red, s_out);
-            cta_allreduce<1>(f1v, ops1, s_red, s_out);
+            cta_allreduce<2, kBW>(d, ops2, s_red, s_out);
+            cta_allreduce<3, kBW>(e3, ops3, s_red, s_out);
+            cta_allreduce<1, kBW>(f1v, ops1, s_red, s_out);
             double a = 0.0, b = d[0], c_term = 0.0, d_term = 0.0;
             if (m > 0) a = lA * d[1] - 2.0 * e3[0];
             if (S.q_is_diag) {
@@ -926,7 +926,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
                 auto f = [&](double xp) {
                     double t[1] = {0.0};
                     for (int i = tid; i < n; i += kBT) t[0] += V.ATdy[i] * (V.QATdy[i] / (1.0 + xp * V.diag_Q[i]));
-                    cta_allreduce<1>(t, ops1, s_red, s_out);
+                    cta_allreduce<1, kBW>(t, ops1, s_red, s_out);
                     return a * xp + b / xp + xp * xp * t[0];
                 };
                 double x1 = right - phi * (right - left), x2 = left + phi * (right - left);
@@ -1013,7 +1013,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_solve(const BatchArgs
             }
             for (int i = tid; i < m; i += kBT) V.y[i] = V.last_y[i] = V.y_bar[i];
             if (m > 0) {
-                cta_spmv(AT, V.y_bar, [&](int i, double s) { V.ATy_bar[i] = V.ATy[i] = V.last_ATy[i] = s; });
+                cta_spmv<kBT>(AT, V.y_bar, [&](int i, double s) { V.ATy_bar[i] = V.ATy[i] = V.last_ATy[i] = s; });
             }
             __syncthreads();
             if (tid == 0) {
@@ -1233,8 +1233,10 @@ struct AdjArgs {
 constexpr int kAdjGlobalN = 5, kAdjGlobalM = 4;  // sol, w_old, w, w_new (+ Q v) per CTA in global memory
 constexpr int kAdjLanczos = 3;                   // v_old, v, v_new (n and m parts)
 
-__global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_adjoint(const AdjArgs B)
+template <int BT>
+__global__ void __launch_bounds__(BT, ctas_per_sm(BT)) k_batch_adjoint(const AdjArgs B)
 {
+    constexpr int kBT = BT, kBW = BT / 32;
     extern __shared__ __align__(16) double dyn_smem[];
     __shared__ double s_red[kBW][8];
     __shared__ double s_out[8];
@@ -1278,7 +1280,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_adjoint(const AdjArgs
             b2[0] += rhs * rhs;
             sol_m[r] = vo_m[r] = wo_m[r] = w_m[r] = 0.0;
         }
-        cta_allreduce<1>(b2, ops1, s_red, s_out);
+        cta_allreduce<1, kBW>(b2, ops1, s_red, s_out);
         const double beta0 = sqrt(b2[0]);
         double beta = beta0, eta = beta0;
         double c_old = 1.0, c = 1.0, s_old = 0.0, s = 0.0;
@@ -1294,18 +1296,18 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_adjoint(const AdjArgs
                 // cta_spmv calls their epilogues for row i on the same thread
                 // and tmp[i] is written and read by that thread.
                 if (m > 0) {
-                    cta_spmv(Q, v_n, [&](int i, double q) { tmp[i] = q; });
-                    cta_spmv(A, v_n, [&](int r, double a) { vn_m[r] = yk[r] != 0.0 ? a : 0.0; });
-                    cta_spmv(AT, v_m,
+                    cta_spmv<kBT>(Q, v_n, [&](int i, double q) { tmp[i] = q; });
+                    cta_spmv<kBT>(A, v_n, [&](int r, double a) { vn_m[r] = yk[r] != 0.0 ? a : 0.0; });
+                    cta_spmv<kBT>(AT, v_m,
                              [&](int i, double at) { vn_n[i] = zk[i] == 0.0 ? tmp[i] + at : 0.0; });
                 } else {
-                    cta_spmv(Q, v_n, [&](int i, double q) { vn_n[i] = zk[i] == 0.0 ? q : 0.0; });
+                    cta_spmv<kBT>(Q, v_n, [&](int i, double q) { vn_n[i] = zk[i] == 0.0 ? q : 0.0; });
                 }
                 __syncthreads();
                 double al[1] = {0.0};
                 for (int i = tid; i < n; i += kBT) al[0] += v_n[i] * vn_n[i];
                 for (int r = tid; r < m; r += kBT) al[0] += v_m[r] * vn_m[r];
-                cta_allreduce<1>(al, ops1, s_red, s_out);
+                cta_allreduce<1, kBW>(al, ops1, s_red, s_out);
                 const double alpha = al[0];
                 double bn[1] = {0.0};
                 for (int i = tid; i < n; i += kBT) {
@@ -1318,7 +1320,7 @@ __global__ void __launch_bounds__(kBT, kCtasPerSm) k_batch_adjoint(const AdjArgs
                     vn_m[r] = t;
                     bn[0] += t * t;
                 }
-                cta_allreduce<1>(bn, ops1, s_red, s_out);
+                cta_allreduce<1, kBW>(bn, ops1, s_red, s_out);
                 const double beta_new = sqrt(bn[0]);
                 // Givens QR of the new tridiagonal column
                 const double r1h = c * alpha - c_old * s * beta;
@@ -1430,6 +1432,7 @@ using HostVec = std::vector<T, NoInitAlloc<T>>;
 struct HPRQPBatch {
     int device = 0;
     int num_sms = 148;
+    int cta_threads = 1024;  // threads per CTA of the solve and adjoint kernels (kBigCta or kSmallCta)
     cudaStream_t stream = nullptr;
     size_t K = 0;
     std::vector<size_t> var_off, row_off;          // original packing (caller's layout)
@@ -1542,7 +1545,7 @@ static void batch_free(HPRQPBatch *b)
 // in arbitrary units: a pass costs half a round and a chunk four rounds.
 constexpr double kRoundCost = 23.1, kShuffleCost = 0.59, kPassCost = 11.6, kChunkCost = 94.3;
 
-static double lane_group_cost(const size_t *rp, int nrow, int lg)
+static double lane_group_cost(const size_t *rp, int nrow, int lg, int kBW)
 {
     const int g = 1 << lg, rpp = 32 >> lg;
     const int per = (nrow + kBW - 1) / kBW;
@@ -1566,12 +1569,12 @@ static double lane_group_cost(const size_t *rp, int nrow, int lg)
     return worst;
 }
 
-static int choose_lane_group(const size_t *rp, int nrow)
+static int choose_lane_group(const size_t *rp, int nrow, int warps)
 {
     int best = 0;
     double best_cost = 0.0;
     for (int lg = 0; lg <= 5; ++lg) {
-        const double c = lane_group_cost(rp, nrow, lg);
+        const double c = lane_group_cost(rp, nrow, lg, warps);
         if (lg == 0 || c <= best_cost) {
             best = lg;
             best_cost = c;
@@ -1640,6 +1643,11 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         return HPRQP_STATUS_NOT_IMPLEMENTED;
     }
     if (device_number < 0 || device_number >= ndev) return HPRQP_STATUS_INVALID_ARGUMENT;
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_number) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
 
     const char *trc = getenv("HPRQP_B200_BATCH_TRACE");
     const bool ctrace = trc && trc[0] == '1';
@@ -1648,6 +1656,9 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     HPRQPBatch *b = new HPRQPBatch();
     b->K = K;
     b->device = device_number;
+    // 512-thread CTAs (two per SM) when one wave of them holds the whole
+    // batch and one wave of 1024-thread CTAs does not
+    b->cta_threads = (K > (size_t)sms && K <= (size_t)2 * sms) ? kSmallCta : kBigCta;
     b->var_off.assign(var_offsets, var_offsets + K + 1);
     b->row_off.assign(row_offsets, row_offsets + K + 1);
     b->total_m_orig = A->nrow;
@@ -1768,9 +1779,9 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     for (size_t k = tix; k < K; k += nth) {
         const HPRQPModel &M = b->models[k];
         BInst &I = b->inst[k];
-        I.q_lg = b->tuned_lg[3 * k] = choose_lane_group(M.Q.row_ptr, (int)M.Q.nrow);
-        I.a_lg = b->tuned_lg[3 * k + 1] = choose_lane_group(M.A.row_ptr, (int)M.A.nrow);
-        I.at_lg = b->tuned_lg[3 * k + 2] = choose_lane_group(M.AT.row_ptr, (int)M.AT.nrow);
+        I.q_lg = b->tuned_lg[3 * k] = choose_lane_group(M.Q.row_ptr, (int)M.Q.nrow, b->cta_threads / 32);
+        I.a_lg = b->tuned_lg[3 * k + 1] = choose_lane_group(M.A.row_ptr, (int)M.A.nrow, b->cta_threads / 32);
+        I.at_lg = b->tuned_lg[3 * k + 2] = choose_lane_group(M.AT.row_ptr, (int)M.AT.nrow, b->cta_threads / 32);
         for (size_t r = 0; r <= M.Q.nrow; ++r) h_qrp[I.q_rp + r] = (int)M.Q.row_ptr[r];
         for (size_t r = 0; r <= M.A.nrow; ++r) h_arp[I.a_rp + r] = (int)M.A.row_ptr[r];
         for (size_t r = 0; r <= M.AT.nrow; ++r) h_atrp[I.at_rp + r] = (int)M.AT.row_ptr[r];
@@ -1910,11 +1921,13 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     BatchArgs &G = b->args;
     const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
     const size_t vec_bytes = (4 * na + 2 * ma) * sizeof(double);  // the gathered vectors
-    G.vec_smem = HPR_BATCH_VEC_SMEM && vec_bytes <= kSmemLimit;
+    const int bt = b->cta_threads;
+    auto kern = bt == kBigCta ? k_batch_solve<kBigCta> : k_batch_solve<kSmallCta>;
+    G.vec_smem = HPR_BATCH_VEC_SMEM && vec_bytes <= smem_limit(bt);
     const size_t smem = G.vec_smem ? vec_bytes : 0;
-    B_CK(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    B_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve, kBT, smem));
+    B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, bt, smem));
     const int grid = std::max(1, std::min((int)b->K, b->num_sms * std::max(per_sm, 1)));
     // per-CTA workspace (allocated lazily, sized by the grid)
     const size_t stride = kBatchNVecs * na + kBatchMVecs * ma;
@@ -1954,7 +1967,7 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
         B_CK(cudaMemsetAsync(d_phase, 0, (size_t)grid * 8 * sizeof(unsigned long long), b->stream));
     }
     G.phase_clk = d_phase;
-    k_batch_solve<<<grid, kBT, smem, b->stream>>>(G);
+    kern<<<grid, bt, smem, b->stream>>>(G);
     count_launch();
     cudaEventRecord(e1, b->stream);
     cudaError_t err = cudaEventSynchronize(e1);
@@ -2149,11 +2162,13 @@ HPRQPStatus hprqp_batch_backward(HPRQPBatch *b, const double *grad_x, const doub
     // ---- device buffers (first call only)
     const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
     const size_t lz_bytes = (size_t)kAdjLanczos * (na + ma) * sizeof(double);
-    const int lanczos_smem = lz_bytes <= kSmemLimit;
+    const int bt = b->cta_threads;
+    auto kern = bt == kBigCta ? k_batch_adjoint<kBigCta> : k_batch_adjoint<kSmallCta>;
+    const int lanczos_smem = lz_bytes <= smem_limit(bt);
     const size_t smem = lanczos_smem ? lz_bytes : 0;
-    B_CK(cudaFuncSetAttribute(k_batch_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    B_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_adjoint, kBT, smem));
+    B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, bt, smem));
     const int grid = std::max(1, std::min((int)K, b->num_sms * std::max(per_sm, 1)));
     const size_t stride = kAdjGlobalN * na + kAdjGlobalM * ma + (lanczos_smem ? 0 : (size_t)kAdjLanczos * (na + ma));
     if (!b->adj_gx) {
@@ -2216,7 +2231,7 @@ HPRQPStatus hprqp_batch_backward(HPRQPBatch *b, const double *grad_x, const doub
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, b->stream);
-    k_batch_adjoint<<<grid, kBT, smem, b->stream>>>(A);
+    kern<<<grid, bt, smem, b->stream>>>(A);
     count_launch();
     cudaEventRecord(e1, b->stream);
     cudaError_t err = cudaEventSynchronize(e1);

@@ -130,6 +130,36 @@ def test_single_adjoint_large_kkt_residual(engine_lib):
     assert np.all(g["lam"][r.z != 0.0] == 0.0) and np.all(g["mu"][r.y == 0.0] == 0.0)
 
 
+def test_single_adjoint_at_large_qp_size_converges(engine_lib):
+    """The single large backward at the large QP's sizes (n = 1e6, m = 5e5,
+    nnz(A) = 1e7, nnz(Q) ~ 3.2e7; the plain recipe, whose forward reaches
+    1e-8): the forward solve is OPTIMAL, MINRES reaches a relative residual
+    of 1e-10, and the adjoint satisfies the active-set KKT system assembled
+    on the host to 1e-7 relative (MINRES runs on the scaled system)."""
+    import scipy.sparse as sp
+
+    hprqp = engine_lib
+    inst = instances.config1_sized_plain()
+    model = hprqp.build_from_instance(inst)
+    r, state = hprqp.solve_for_backward(model, hprqp.Parameters(verbose=False, stoptol=1e-8, time_limit=300.0))
+    assert r.status_code == hprqp.STATUS_OPTIMAL and r.residual < 1e-8
+    assert state is not None
+    try:
+        gx = np.random.default_rng(1).standard_normal(inst.n)
+        g = state.backward(gx, tol=1e-10, max_iter=50000)
+    finally:
+        state.close()
+    assert g["minres_relres"] <= 1e-10, g["minres_relres"]
+    mi = _model_instance(hprqp, model)
+    F = np.nonzero(r.z == 0.0)[0]
+    R = np.nonzero(r.y != 0.0)[0]
+    Q = mi.Q.to_scipy()
+    A = mi.A.to_scipy()
+    AF = A[R][:, F]
+    res = np.concatenate([Q[F][:, F] @ g["lam"][F] + AF.T @ g["mu"][R] - gx[F], AF @ g["lam"][F]])
+    assert np.linalg.norm(res) <= 1e-7 * np.linalg.norm(gx[F]), np.linalg.norm(res) / np.linalg.norm(gx[F])
+
+
 def test_torch_single_qp_function_matches_batched_layer(engine_lib):
     """hprqp.SingleQPFunction (solve_gpu + device-wide adjoint) and the
     batched QPFunction give the same gradients for the same QP, on CUDA

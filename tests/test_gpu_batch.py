@@ -103,6 +103,30 @@ def test_batch_spmv_lane_widths(engine_lib, lanes, cap):
                 assert np.max(np.abs(got - ref)) <= 1e-12 * max(1.0, float(np.max(np.abs(ref)))), (inst.name, lanes)
 
 
+def test_batch_between_one_and_two_instances_per_sm(engine_lib):
+    """A batch of more instances than SMs but at most two per SM runs on
+    512-thread CTAs (one wave, two per SM) instead of 1024-thread ones: the
+    fixture models repeated to 13 x 12 = 156 instances give the oracle's
+    status, iteration count and iterates within 1e-12 after 10 steps."""
+    from hprqp import batch
+
+    tiny = instances.tiny_cases()
+    insts = tiny * 13
+    assert 148 < len(insts) <= 296
+    b = batch.Batch(insts)
+    b.solve(stoptol=1e-8, max_iter=10)
+    r = b.results()
+    b.close()
+    xs, ys = b.split(r.x, "x"), b.split(r.y, "y")
+    ref = {}
+    for k, inst in enumerate(insts):
+        o = ref.setdefault(inst.name, pyoracle.OracleModel(inst).solve(stoptol=1e-8, max_iter=10,
+                                                                       mode=pyoracle.MODE_GPU_REF))
+        assert r.status[k] == o["status"] and r.iter[k] == o["iter"], inst.name
+        for got, want in ((xs[k], o["x"]), (ys[k][_kept(inst)], o["y"])):
+            assert len(want) == 0 or np.max(np.abs(got - want)) <= 1e-12, inst.name
+
+
 def test_batch_spmv_lanes_rejects_bad_width(engine_lib):
     from hprqp import batch
 
