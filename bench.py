@@ -41,12 +41,13 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "hpr-qp-c_b200" / "python"))
 sys.path.insert(0, str(ROOT / "oracle"))
 
-# DRAM bytes moved per algorithmic byte by k_batch_solve: ncu on a 296-QP
-# launch of this workload (two 512-thread CTAs per SM, one instance each)
-# read+wrote 373.270 GB (dram__bytes_read.sum + dram__bytes_write.sum) for
-# 504.759 GB of algorithmic bytes; the 296 concurrent instances' matrices
-# and vectors no longer all fit in L2, so part of each iteration re-reads HBM.
-BATCH_DRAM_PER_ALGO_BYTE = 373.270e9 / 504.759e9
+# DRAM bytes moved per algorithmic byte by k_batch_solve: ncu on a 300-QP
+# launch of this workload in the bench's kernel shape (1024-thread CTAs, one
+# instance per SM at a time) read+wrote 359.478 + 26.820 GB
+# (dram__bytes_read.sum + dram__bytes_write.sum) for 512.257 GB of
+# algorithmic bytes; traffic grows with instance-iterations, so the bench
+# scales this ratio by its own launch's algorithmic bytes.
+BATCH_DRAM_PER_ALGO_BYTE = 386.298e9 / 512.257e9
 METRIC = "solves/s to 1e-6 rel-KKT, batched vs plain on 1 B200; SpMV GB/s vs HBM peak"
 STOPTOL = 1e-6
 BATCH = 4096
@@ -713,8 +714,8 @@ def main():
                     "optimal": e2e_ok},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": algo_bytes * BATCH_DRAM_PER_ALGO_BYTE,
-                         "traffic_source": "ncu DRAM bytes of a 296-QP launch of this workload, scaled by "
-                                           "algorithmic bytes (instance-iterations)",
+                         "traffic_source": "ncu DRAM bytes of a 300-QP launch of this workload (same kernel "
+                                           "shape), scaled by algorithmic bytes (instance-iterations)",
                          "kernel": "k_batch_solve",
                          "algorithmic_bytes_per_launch": algo_bytes, "peak_kind": peak_kind},
             "solved_optimal": int(np.sum(res.status == 6)), "mean_iters": float(iters.mean())}
