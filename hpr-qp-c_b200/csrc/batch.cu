@@ -1624,8 +1624,11 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
                                      const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c,
                                      const double *AL, const double *AU, const double *l, const double *u,
                                      const double *obj_constants, int device_number, bool keep_caller_csr,
-                                     HPRQPBatch **out, bool abortable = true)
+                                     HPRQPBatch **out, bool abortable = true, size_t k_begin = 0,
+                                     size_t k_count = 0, int cta_threads = 0)
 {
+    // instances [k_begin, k_begin + k_count) of the caller's batch (k_count 0:
+    // all of them); the batch keeps its offsets relative to its first one
     using namespace hpr;
     if (!out || !var_offsets || !row_offsets || !Q || !A || !c || !l || !u || K == 0)
         return HPRQP_STATUS_INVALID_ARGUMENT;
@@ -1637,6 +1640,11 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     for (size_t k = 0; k < K; ++k)
         if (var_offsets[k + 1] < var_offsets[k] || row_offsets[k + 1] < row_offsets[k])
             return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (k_count == 0) k_count = K - k_begin;
+    if (k_begin >= K || k_count > K - k_begin || (keep_caller_csr && k_count != K))
+        return HPRQP_STATUS_INVALID_ARGUMENT;
+    const size_t kb = k_begin;
+    K = k_count;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         fprintf(stderr, "hprqp-b200: no CUDA device available; this engine has no CPU fallback\n");
@@ -1659,9 +1667,14 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     // 512-thread CTAs (two per SM) when one wave of them holds the whole
     // batch and one wave of 1024-thread CTAs does not
     b->cta_threads = (K > (size_t)sms && K <= (size_t)2 * sms) ? kSmallCta : kBigCta;
-    b->var_off.assign(var_offsets, var_offsets + K + 1);
-    b->row_off.assign(row_offsets, row_offsets + K + 1);
-    b->total_m_orig = A->nrow;
+    if (cta_threads == kSmallCta || cta_threads == kBigCta) b->cta_threads = cta_threads;
+    b->var_off.resize(K + 1);
+    b->row_off.resize(K + 1);
+    for (size_t k = 0; k <= K; ++k) {
+        b->var_off[k] = var_offsets[kb + k] - var_offsets[kb];
+        b->row_off[k] = row_offsets[kb + k] - row_offsets[kb];
+    }
+    b->total_m_orig = row_offsets[kb + K] - row_offsets[kb];
     b->models.resize(K);
     for (auto &mm : b->models) model_init(&mm);
     b->kept_rows.resize(K);
@@ -1679,7 +1692,8 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         std::vector<size_t> qrp, qci, arp, aci;
         std::vector<double> qv, av;
         for (size_t k = tix; k < K; k += nth) {
-            const size_t v0 = var_offsets[k], v1 = var_offsets[k + 1], r0 = row_offsets[k], r1 = row_offsets[k + 1];
+            const size_t v0 = var_offsets[kb + k], v1 = var_offsets[kb + k + 1], r0 = row_offsets[kb + k],
+                         r1 = row_offsets[kb + k + 1];
             HPRQPStatus st = extract_block(Q, v0, v1, v0, v1, qrp, qci, qv);
             if (st == HPRQP_STATUS_OK) st = extract_block(A, r0, r1, v0, v1, arp, aci, av);
             if (st != HPRQP_STATUS_OK) {
@@ -1693,7 +1707,7 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
             HPRQPMatrixCSR a{r1 - r0, v1 - v0, aci.size(), arp.data(), aci.empty() ? &e_idx : aci.data(),
                              av.empty() ? &e_val : av.data(), 0};
             st = build_from_QAbc(&q, &a, c + v0, r1 > r0 ? AL + r0 : nullptr, r1 > r0 ? AU + r0 : nullptr, l + v0,
-                                 u + v0, obj_constants ? obj_constants[k] : 0.0, &b->models[k]);
+                                 u + v0, obj_constants ? obj_constants[kb + k] : 0.0, &b->models[k]);
             st_k[k] = st;
             if (st == HPRQP_STATUS_OK) {
                 // record which original rows survived preprocessing
@@ -1913,10 +1927,22 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
                              out);
 }
 
-HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
+}  // extern "C"
+
+namespace hpr {
+
+// a launched solve (batch_launch) waiting for batch_finish
+struct SolveLaunch {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    unsigned long long *d_phase = nullptr;
+    int grid = 0;
+    size_t smem = 0;
+};
+
+// Start the solve kernel of a batch on its stream and return; the kernel's
+// events and optional phase clocks are in L.
+static HPRQPStatus batch_launch(HPRQPBatch *b, const HPRQPBatchParams *p, SolveLaunch &L)
 {
-    using namespace hpr;
-    if (!b || !p) return HPRQP_STATUS_INVALID_ARGUMENT;
     B_CK(cudaSetDevice(b->device));
     BatchArgs &G = b->args;
     const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
@@ -1952,7 +1978,7 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     B_CK(cudaMemcpyAsync(&h_t0, d_t0, sizeof(h_t0), cudaMemcpyDeviceToHost, b->stream));
     B_CK(cudaStreamSynchronize(b->stream));
     G.t_start = h_t0;
-    cudaEvent_t e0, e1;
+    cudaEvent_t &e0 = L.e0, &e1 = L.e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, b->stream);
@@ -1970,6 +1996,21 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     kern<<<grid, bt, smem, b->stream>>>(G);
     count_launch();
     cudaEventRecord(e1, b->stream);
+    L.d_phase = d_phase;
+    L.grid = grid;
+    L.smem = smem;
+    return HPRQP_STATUS_OK;
+}
+
+// Wait for a launched solve, record its device time, print the optional
+// phase clocks.
+static HPRQPStatus batch_finish(HPRQPBatch *b, SolveLaunch &L)
+{
+    cudaEvent_t e0 = L.e0, e1 = L.e1;
+    unsigned long long *d_phase = L.d_phase;
+    const int grid = L.grid;
+    const size_t smem = L.smem;
+    B_CK(cudaSetDevice(b->device));
     cudaError_t err = cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
@@ -1993,6 +2034,24 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
                 100 * tot[4] / tot[7], 100 * tot[5] / tot[7], 100 * tot[6] / tot[7], grid, smem);
     }
     return HPRQP_STATUS_OK;
+}
+
+}  // namespace hpr
+
+extern "C" {
+
+HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
+{
+    using namespace hpr;
+    if (!b || !p) return HPRQP_STATUS_INVALID_ARGUMENT;
+    SolveLaunch L;
+    HPRQPStatus st = batch_launch(b, p, L);
+    if (st != HPRQP_STATUS_OK) {
+        if (L.e0) cudaEventDestroy(L.e0);
+        if (L.e1) cudaEventDestroy(L.e1);
+        return st;
+    }
+    return batch_finish(b, L);
 }
 
 HPRQPStatus hprqp_batch_set_warm_start(HPRQPBatch *b, const double *x0, const double *y0, const double *w0,
@@ -2324,6 +2383,89 @@ void hprqp_batch_destroy(HPRQPBatch *b)
     delete b;
 }
 
+}  // extern "C"
+
+namespace hpr {
+
+// The one-call form of a large batch in two launches, so that the host's
+// preprocessing and upload of the second part run while the GPU solves the
+// first: the first part (about a quarter of the work, by nonzeros) is built
+// and launched, the rest is built and uploaded meanwhile and launched on its
+// own stream (its CTAs take the SMs as the first launch's CTAs finish), and
+// the results of both land in the caller's arrays.  Each instance is solved
+// by one CTA of the shape a single launch would use (batches this large take
+// 1024-thread CTAs), so the results equal a single launch's bit for bit;
+// each launch keeps its own time limit.
+constexpr size_t kSplitMinInstances = 1024;
+
+static HPRQPStatus solve_batch_in_two(size_t K, const size_t *var_offsets, const size_t *row_offsets,
+                                      const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c,
+                                      const double *AL, const double *AU, const double *l, const double *u,
+                                      const double *obj_constants, const HPRQPBatchParams *params, int *status,
+                                      size_t *iter, double *primal_obj, double *residual, double *gap, double *x,
+                                      double *y, double *z, double *w, bool trace)
+{
+    auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    const double t0 = now();
+    // split where the nonzeros of the first part reach a quarter of the total
+    auto weight = [&](size_t k) {
+        const size_t v0 = var_offsets[k], v1 = var_offsets[k + 1], r0 = row_offsets[k], r1 = row_offsets[k + 1];
+        return (double)(Q->row_ptr[v1] - Q->row_ptr[v0]) + 2.0 * (double)(A->row_ptr[r1] - A->row_ptr[r0]) +
+               (double)(v1 - v0);
+    };
+    double total = 0.0;
+    for (size_t k = 0; k < K; ++k) total += weight(k);
+    size_t K1 = 0;
+    for (double acc = 0.0; K1 < K - 1 && acc < 0.25 * total; ++K1) acc += weight(K1);
+    K1 = std::max<size_t>(K1, 1);
+    HPRQPBatch *b[2] = {nullptr, nullptr};
+    SolveLaunch L[2];
+    HPRQPStatus st = HPRQP_STATUS_OK;
+    const size_t first[2] = {0, K1}, count[2] = {K1, K - K1};
+    int launched = 0;
+    double t_create[2] = {0.0, 0.0};
+    for (int part = 0; part < 2 && st == HPRQP_STATUS_OK; ++part) {
+        const double tc = now();
+        // both parts take the CTA shape the whole batch would take, so each
+        // instance sums in the same order as in a single launch
+        st = batch_create_impl(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants,
+                               params->device_number, false, &b[part], false, first[part], count[part], kBigCta);
+        t_create[part] = now() - tc;
+        if (st == HPRQP_STATUS_OK) st = batch_launch(b[part], params, L[part]);
+        if (st == HPRQP_STATUS_OK) ++launched;
+    }
+    const double t1 = now();
+    for (int part = 0; part < launched; ++part) {
+        const HPRQPStatus s2 = batch_finish(b[part], L[part]);
+        if (st == HPRQP_STATUS_OK) st = s2;
+    }
+    const double t2 = now();
+    for (int part = 0; part < 2 && st == HPRQP_STATUS_OK; ++part) {
+        const size_t kb = first[part], v0 = var_offsets[kb], r0 = row_offsets[kb];
+        st = hprqp_batch_get_results(b[part], status ? status + kb : nullptr, iter ? iter + kb : nullptr,
+                                     primal_obj ? primal_obj + kb : nullptr, residual ? residual + kb : nullptr,
+                                     gap ? gap + kb : nullptr, x ? x + v0 : nullptr, y ? y + r0 : nullptr,
+                                     z ? z + v0 : nullptr, w ? w + v0 : nullptr);
+    }
+    const double t3 = now();
+    for (int part = 0; part < 2; ++part) {
+        if (part >= launched && L[part].e0) cudaEventDestroy(L[part].e0);
+        if (part >= launched && L[part].e1) cudaEventDestroy(L[part].e1);
+        if (b[part]) hprqp_batch_destroy(b[part]);
+    }
+    if (trace)
+        fprintf(stderr,
+                "[hprqp-b200 batch] in two launches (%zu + %zu instances): create %.3f + %.3f s, until both kernels "
+                "end %.3f s, results %.3f s, destroy %.3f s\n",
+                count[0], count[1], t_create[0], t_create[1], t2 - t1 + (t1 - t0 - t_create[0] - t_create[1]),
+                t3 - t2, now() - t3);
+    return st;
+}
+
+}  // namespace hpr
+
+extern "C" {
+
 HPRQPStatus hprqp_solve_batch(size_t K, const size_t *var_offsets, const size_t *row_offsets, const HPRQPMatrixCSR *Q,
                               const HPRQPMatrixCSR *A, const double *c, const double *AL, const double *AU,
                               const double *l, const double *u, const double *obj_constants,
@@ -2335,6 +2477,10 @@ HPRQPStatus hprqp_solve_batch(size_t K, const size_t *var_offsets, const size_t 
     const bool trace = tr && tr[0] == '1';
     auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
     const double t0 = now();
+    if (K >= hpr::kSplitMinInstances && Q && A && var_offsets && row_offsets && matrix_csr_is_valid(Q) &&
+        matrix_csr_is_valid(A) && var_offsets[K] == Q->nrow && row_offsets[K] == A->nrow)
+        return hpr::solve_batch_in_two(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants, params,
+                                       status, iter, primal_obj, residual, gap, x, y, z, w, trace);
     HPRQPBatch *b = nullptr;
     HPRQPStatus st = batch_create_impl(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants,
                                        params->device_number, false, &b, false);

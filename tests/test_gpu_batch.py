@@ -207,3 +207,58 @@ def test_batch_noc_and_empty_rows(engine_lib):
         assert abs(r.objective[k] - o["primal_obj"]) <= 1e-6 * max(1.0, abs(o["primal_obj"]))
     ys = np.split(r.y, np.cumsum([i.m for i in insts])[:-1])
     assert ys[1][3] == 0.0 and len(ys[1]) == holes.m
+
+
+def _one_call(hprqp, packed, **kw):
+    """hprqp_solve_batch (create + solve + results + destroy in one call)."""
+    import ctypes
+
+    from hprqp import batch as hb
+
+    lib = hprqp._lib()
+    hb._configure()
+    fn = lib.hprqp_solve_batch
+    szp, dbp = ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_double)
+    fn.argtypes = [ctypes.c_size_t, szp, szp, ctypes.POINTER(hprqp._MatrixCSR), ctypes.POINTER(hprqp._MatrixCSR),
+                   dbp, dbp, dbp, dbp, dbp, dbp, ctypes.POINTER(hb.BatchParams), ctypes.POINTER(ctypes.c_int), szp,
+                   dbp, dbp, dbp, dbp, dbp, dbp, dbp]
+    p = packed
+    n, m = int(p.var_offsets[-1]), int(p.row_offsets[-1])
+    keep = []
+    Q = hb._csr(n, n, p.q_indptr, p.q_indices, p.q_data, keep)
+    A = hb._csr(m, n, p.a_indptr, p.a_indices, p.a_data, keep)
+    dp = lambda a: a.ctypes.data_as(dbp)  # noqa: E731
+    out = dict(status=np.zeros(p.K, np.int32), iter=np.zeros(p.K, np.uint64), obj=np.zeros(p.K),
+               res=np.zeros(p.K), gap=np.zeros(p.K), x=np.zeros(n), y=np.zeros(max(m, 1)), z=np.zeros(n),
+               w=np.zeros(n))
+    vo = np.ascontiguousarray(p.var_offsets, np.uint64)
+    ro = np.ascontiguousarray(p.row_offsets, np.uint64)
+    params = hb.default_params(**kw)
+    st = fn(p.K, vo.ctypes.data_as(szp), ro.ctypes.data_as(szp), ctypes.byref(Q), ctypes.byref(A), dp(p.c),
+            dp(p.AL), dp(p.AU), dp(p.l), dp(p.u), dp(p.obj), ctypes.byref(params),
+            out["status"].ctypes.data_as(ctypes.POINTER(ctypes.c_int)), out["iter"].ctypes.data_as(szp),
+            dp(out["obj"]), dp(out["res"]), dp(out["gap"]), dp(out["x"]), dp(out["y"]), dp(out["z"]), dp(out["w"]))
+    assert st == hprqp.STATUS_OK
+    out["y"] = out["y"][:m]
+    return out
+
+
+@pytest.mark.parametrize("count", [12, 1100])
+def test_one_call_equals_batch_handle(engine_lib, count):
+    """hprqp_solve_batch gives bit for bit what a Batch handle gives on the
+    same instances -- also for batches large enough that the one-call form
+    builds and launches them in two parts (1100 >= 1024 instances)."""
+    from hprqp import batch
+
+    insts = [instances.config4_instance(i) for i in range(count)]
+    packed = batch.pack(insts)
+    one = _one_call(engine_lib, packed, stoptol=1e-6)
+    b = batch.Batch(packed)
+    b.solve(stoptol=1e-6)
+    r = b.results()
+    b.close()
+    assert np.array_equal(one["status"], r.status) and np.all(r.status == 6)
+    assert np.array_equal(one["iter"].astype(np.int64), r.iter)
+    assert np.array_equal(one["obj"], r.objective)
+    for key, ref in (("x", r.x), ("y", r.y), ("z", r.z), ("w", r.w)):
+        assert np.array_equal(one[key], ref), key
