@@ -1,8 +1,9 @@
 // Batched HPR-QP solver: one persistent kernel solves thousands of
 // independent QPs.
 //
-// Each CTA takes instances from a global work queue (largest first, so the
-// tail of the batch is made of short jobs) and runs the complete method for
+// Each CTA takes instances from a global work queue with two ends (even
+// CTAs take the largest instance left, odd CTAs the smallest, take_instance)
+// and runs the complete method for
 // its instance: Ruiz + Pock-Chambolle scaling, power iterations, HPR steps,
 // residual checks, restarts and the sigma update, with the control logic of
 // the reference's outer loop (src/shared/solver_backend.c:338-569,
@@ -74,7 +75,7 @@ struct BatchArgs {
     int K;
     const BInst *inst;
     const int *order;
-    int *counter;
+    unsigned long long *counter;  // the work queue's two ends (take_instance)
     const int *q_rp, *q_ci, *a_rp, *a_ci, *at_rp, *at_ci;
     const double *q_v0, *a_v0, *at_v0, *c0, *l0, *u0, *AL0, *AU0;
     double *q_v, *a_v, *at_v;  // scaled copies
@@ -354,15 +355,18 @@ static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q,
     __syncthreads();
     cta_allreduce<1, kBW>(v1, ops1, s_red, s_out);
     double zz = v1[0], lambda = 1.0;
+    bool q_ready = false;  // q = z / |z| was already written by the last residual pass
     for (int it = 0; it < 5000; ++it) {
         const double qn = sqrt(zz);
         if (qn <= 1e-16) {
             lambda = 0.0;
             break;
         }
-        const double inv = 1.0 / qn;
-        for (int i = tid; i < len; i += kBT) q[i] = z[i] * inv;
-        __syncthreads();
+        if (!q_ready) {
+            const double inv = 1.0 / qn;
+            for (int i = tid; i < len; i += kBT) q[i] = z[i] * inv;
+            __syncthreads();
+        }
         double v2[2] = {0.0, 0.0};
         const int ops2[2] = {kSum, kSum};
         if (is_a) {
@@ -385,17 +389,40 @@ static __device__ double cta_power(const LCsr &A, const LCsr &AT, const LCsr &Q,
         lambda = v2[0];
         zz = v2[1];
         const double zn = sqrt(zz);
+        // the residual |z - lambda q| and, in the same pass, the next
+        // iteration's q = z / |z| (the same products as a separate pass; not
+        // used when the residual test stops the iteration)
+        q_ready = zn > 1e-16;
+        const double inv_next = q_ready ? 1.0 / zn : 0.0;
         double v3[1] = {0.0};
         for (int i = tid; i < len; i += kBT) {
             const double r = z[i] - lambda * q[i];
-            q[i] = r;
+            if (q_ready) q[i] = z[i] * inv_next;
             v3[0] += r * r;
         }
-        __syncthreads();
         cta_allreduce<1, kBW>(v3, ops1, s_red, s_out);
         if (sqrt(v3[0]) / (zn + fabs(lambda) + 1e-16) < 1e-4) break;
     }
     return lambda < 0.0 ? 0.0 : lambda;
+}
+
+// The next instance for this CTA, or -1 when every instance is taken.
+// `order` lists the instances largest first (nonzeros); even CTAs take from
+// its front, odd CTAs from its back.  Iteration counts vary most among the
+// small instances (a few run a hundred times the median count), and such a
+// straggler taken last would run alone at the end of the launch; from the
+// back it starts at once, while the large instances, whose counts vary
+// little, are still taken largest first.  One 64-bit counter holds both
+// ends (low half: taken from the front, high half: from the back), so one
+// atomic both claims an index and checks that the two ends have not met;
+// the claims that succeed hand out each index exactly once.
+static __device__ __forceinline__ int take_instance(unsigned long long *counter, const int *order, int K)
+{
+    const bool back = blockIdx.x & 1;
+    const unsigned long long old = atomicAdd(counter, back ? (1ull << 32) : 1ull);
+    const unsigned long long front_taken = old & 0xffffffffull, back_taken = old >> 32;
+    if (front_taken + back_taken >= (unsigned long long)K) return -1;
+    return order[back ? K - 1 - (int)back_taken : (int)front_taken];
 }
 
 static __device__ __forceinline__ size_t adaptive_step_d(long long iter)
@@ -442,8 +469,7 @@ __global__ void __launch_bounds__(BT, ctas_per_sm(BT)) k_batch_solve(const Batch
 
     for (;;) {
         if (tid == 0) {
-            const int slot = atomicAdd(B.counter, 1);
-            s_inst = slot < B.K ? B.order[slot] : -1;
+            s_inst = take_instance(B.counter, B.order, B.K);
             // an instance taken after the batch's time limit or after an
             // abort request is not set up: it reports TIME_LIMIT at iteration
             // 0 with zero vectors and infinite residuals
@@ -1214,7 +1240,7 @@ struct AdjArgs {
     int K;
     const BInst *inst;
     const int *order;
-    int *counter;
+    unsigned long long *counter;  // the work queue's two ends (take_instance)
     const int *q_rp, *q_ci, *a_rp, *a_ci, *at_rp, *at_ci;
     const double *q_v, *a_v, *at_v;             // scaled matrices left by the last solve
     const double *col_norm, *row_norm, *z, *y;  // per instance, packed
@@ -1247,8 +1273,7 @@ __global__ void __launch_bounds__(BT, ctas_per_sm(BT)) k_batch_adjoint(const Adj
     double *lz = B.lanczos_smem ? dyn_smem : g + kAdjGlobalN * (size_t)na + kAdjGlobalM * (size_t)ma;
     for (;;) {
         if (tid == 0) {
-            const int slot = atomicAdd(B.counter, 1);
-            s_inst = slot < B.K ? B.order[slot] : -1;
+            s_inst = take_instance(B.counter, B.order, B.K);
         }
         __syncthreads();
         const int k = s_inst;
@@ -1454,7 +1479,8 @@ struct HPRQPBatch {
     // adjoint buffers, allocated by the first hprqp_batch_backward
     double *adj_gx = nullptr, *adj_gy = nullptr, *adj_lx = nullptr, *adj_ly = nullptr, *adj_rel = nullptr;
     double *adj_ws = nullptr;
-    int *adj_it = nullptr, *adj_counter = nullptr;
+    int *adj_it = nullptr;
+    unsigned long long *adj_counter = nullptr;
     size_t adj_ws_count = 0;
     double last_adjoint_ms = 0.0;
     // warm start (device packing: total variables, kept rows), set by
@@ -1850,7 +1876,8 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     int *d_qrp, *d_arp, *d_atrp, *d_qci, *d_aci, *d_atci;
     double *d_qv0, *d_av0, *d_atv0, *d_c, *d_l, *d_u, *d_AL, *d_AU;
     BInst *d_inst;
-    int *d_order, *d_counter;
+    int *d_order;
+    unsigned long long *d_counter;
     Carver cv;
     cv.add(&d_qrp, qrp).add(&d_arp, arp).add(&d_atrp, atrp).add(&d_qci, h_qci.size()).add(&d_aci, h_aci.size());
     cv.add(&d_atci, h_atci.size()).add(&d_qv0, h_qv.size()).add(&d_av0, h_av.size()).add(&d_atv0, h_atv.size());
@@ -1971,7 +1998,7 @@ static HPRQPStatus batch_launch(HPRQPBatch *b, const HPRQPBatchParams *p, SolveL
     G.print_frequency = p->print_frequency;
     G.use_scaling = p->use_scaling;
     unsigned long long *d_t0 = b->d_t0;
-    B_CK(cudaMemsetAsync(G.counter, 0, sizeof(int), b->stream));
+    B_CK(cudaMemsetAsync(G.counter, 0, sizeof(*G.counter), b->stream));
     k_batch_clock<<<1, 1, 0, b->stream>>>(d_t0);
     count_launch();
     unsigned long long h_t0 = 0;
@@ -2254,7 +2281,7 @@ HPRQPStatus hprqp_batch_backward(HPRQPBatch *b, const double *grad_x, const doub
     for (size_t k = 0; k < K; ++k)
         memcpy(&gx_dev[b->inst[k].var], grad_x + b->var_off[k], (size_t)b->inst[k].n * sizeof(double));
     B_CK(cudaMemcpyAsync(b->adj_gx, gx_dev.data(), N * sizeof(double), cudaMemcpyHostToDevice, b->stream));
-    B_CK(cudaMemsetAsync(b->adj_counter, 0, sizeof(int), b->stream));
+    B_CK(cudaMemsetAsync(b->adj_counter, 0, sizeof(*b->adj_counter), b->stream));
     AdjArgs A{};
     A.K = (int)K;
     A.inst = G.inst;
