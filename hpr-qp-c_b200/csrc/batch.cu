@@ -58,9 +58,11 @@ namespace hpr {
 constexpr int kBigCta = 1024, kSmallCta = 512;
 constexpr int ctas_per_sm(int bt) { return bt >= 1024 ? 1 : 1024 / bt; }
 // dynamic shared memory per CTA: the gathered vectors move to shared memory
-// when they fit (every instance of n, m <= 2000), else they stay in global
-// memory (L1-cached)
+// when they fit and the pool leaves L1 large (batch_launch), else they stay
+// in global memory (L1-cached)
 constexpr size_t smem_limit(int bt) { return ctas_per_sm(bt) == 1 ? 200 * 1024 : 110 * 1024; }
+// shared memory per SM up to which the gathered vectors use a pool (batch_launch)
+constexpr size_t kPoolPerSm = 64 * 1024, kReservedSmemPerCta = 1024;
 
 struct BInst {
     long long q_nz, a_nz, at_nz;  // first entry of the instance's matrices
@@ -641,7 +643,9 @@ __global__ void __launch_bounds__(BT, ctas_per_sm(BT)) k_batch_solve(const Batch
             if (tid == 0) S.lQ = lq * 1.05;
         }
         {
-            const double la = m > 0 ? cta_power<kBT>(A, AT, Q, true, m, V.pz, V.pq, V.pn, s_red, s_out) : 0.0;
+            // the products' sources in the slots of y_bar and w (shared
+            // memory), which the starting iterates below overwrite
+            const double la = m > 0 ? cta_power<kBT>(A, AT, Q, true, m, V.pz, V.y_bar, V.w, s_red, s_out) : 0.0;
             if (tid == 0) S.lA = la * 1.05;
         }
         __syncthreads();
@@ -1976,7 +1980,19 @@ static HPRQPStatus batch_launch(HPRQPBatch *b, const HPRQPBatchParams *p, SolveL
     const size_t vec_bytes = (4 * na + 2 * ma) * sizeof(double);  // the gathered vectors
     const int bt = b->cta_threads;
     auto kern = bt == kBigCta ? k_batch_solve<kBigCta> : k_batch_solve<kSmallCta>;
-    G.vec_smem = HPR_BATCH_VEC_SMEM && vec_bytes <= smem_limit(bt);
+    // The gathered vectors go to shared memory only while the carveout that
+    // takes leaves most of the SM's 256 KB of unified L1 / shared memory to
+    // L1, which holds the instance's other vectors and its matrices: at most
+    // kPoolPerSm bytes of shared memory per SM (static and reserved bytes of
+    // every resident CTA included).  Measured on the 4096-QP batch (n up to
+    // 2000: 99.5 KB per SM with the pool) the pool made the mid-size
+    // instances whose whole working set fits a 248 KB L1 (n ~ 500) 5 % slower
+    // and the large ones 4 % faster; on 296 large QPs (two CTAs per SM, 195
+    // KB) it cost 12 %; on 256 QPs of n = 500 (48 KB) it saved 12 %.
+    cudaFuncAttributes fa;
+    B_CK(cudaFuncGetAttributes(&fa, kern));
+    const size_t pool_per_sm = (size_t)ctas_per_sm(bt) * (vec_bytes + fa.sharedSizeBytes + kReservedSmemPerCta);
+    G.vec_smem = HPR_BATCH_VEC_SMEM && vec_bytes <= smem_limit(bt) && pool_per_sm <= kPoolPerSm;
     const size_t smem = G.vec_smem ? vec_bytes : 0;
     B_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
