@@ -1655,10 +1655,12 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
                                      const double *AL, const double *AU, const double *l, const double *u,
                                      const double *obj_constants, int device_number, bool keep_caller_csr,
                                      HPRQPBatch **out, bool abortable = true, size_t k_begin = 0,
-                                     size_t k_count = 0, int cta_threads = 0)
+                                     size_t k_count = 0, int cta_threads = 0, const size_t *subset = nullptr)
 {
     // instances [k_begin, k_begin + k_count) of the caller's batch (k_count 0:
-    // all of them); the batch keeps its offsets relative to its first one
+    // all of them), or, when subset is given, the k_count instances
+    // subset[0..k_count) (distinct caller indices; k_begin unused); the batch
+    // packs them one after the other in that order
     using namespace hpr;
     if (!out || !var_offsets || !row_offsets || !Q || !A || !c || !l || !u || K == 0)
         return HPRQP_STATUS_INVALID_ARGUMENT;
@@ -1670,10 +1672,18 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     for (size_t k = 0; k < K; ++k)
         if (var_offsets[k + 1] < var_offsets[k] || row_offsets[k + 1] < row_offsets[k])
             return HPRQP_STATUS_INVALID_ARGUMENT;
+    if (subset) {
+        if (k_count == 0 || k_count > K || keep_caller_csr) return HPRQP_STATUS_INVALID_ARGUMENT;
+        for (size_t j = 0; j < k_count; ++j)
+            if (subset[j] >= K) return HPRQP_STATUS_INVALID_ARGUMENT;
+        k_begin = 0;
+    }
     if (k_count == 0) k_count = K - k_begin;
     if (k_begin >= K || k_count > K - k_begin || (keep_caller_csr && k_count != K))
         return HPRQP_STATUS_INVALID_ARGUMENT;
     const size_t kb = k_begin;
+    // the caller's index of instance k of this batch
+    auto caller = [&](size_t k) { return subset ? subset[k] : kb + k; };
     K = k_count;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -1698,13 +1708,14 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     // batch and one wave of 1024-thread CTAs does not
     b->cta_threads = (K > (size_t)sms && K <= (size_t)2 * sms) ? kSmallCta : kBigCta;
     if (cta_threads == kSmallCta || cta_threads == kBigCta) b->cta_threads = cta_threads;
-    b->var_off.resize(K + 1);
-    b->row_off.resize(K + 1);
-    for (size_t k = 0; k <= K; ++k) {
-        b->var_off[k] = var_offsets[kb + k] - var_offsets[kb];
-        b->row_off[k] = row_offsets[kb + k] - row_offsets[kb];
+    b->var_off.assign(K + 1, 0);
+    b->row_off.assign(K + 1, 0);
+    for (size_t k = 0; k < K; ++k) {
+        const size_t kk = caller(k);
+        b->var_off[k + 1] = b->var_off[k] + (var_offsets[kk + 1] - var_offsets[kk]);
+        b->row_off[k + 1] = b->row_off[k] + (row_offsets[kk + 1] - row_offsets[kk]);
     }
-    b->total_m_orig = row_offsets[kb + K] - row_offsets[kb];
+    b->total_m_orig = b->row_off[K];
     b->models.resize(K);
     for (auto &mm : b->models) model_init(&mm);
     b->kept_rows.resize(K);
@@ -1722,8 +1733,8 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         std::vector<size_t> qrp, qci, arp, aci;
         std::vector<double> qv, av;
         for (size_t k = tix; k < K; k += nth) {
-            const size_t v0 = var_offsets[kb + k], v1 = var_offsets[kb + k + 1], r0 = row_offsets[kb + k],
-                         r1 = row_offsets[kb + k + 1];
+            const size_t kk = caller(k);
+            const size_t v0 = var_offsets[kk], v1 = var_offsets[kk + 1], r0 = row_offsets[kk], r1 = row_offsets[kk + 1];
             HPRQPStatus st = extract_block(Q, v0, v1, v0, v1, qrp, qci, qv);
             if (st == HPRQP_STATUS_OK) st = extract_block(A, r0, r1, v0, v1, arp, aci, av);
             if (st != HPRQP_STATUS_OK) {
@@ -1737,7 +1748,7 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
             HPRQPMatrixCSR a{r1 - r0, v1 - v0, aci.size(), arp.data(), aci.empty() ? &e_idx : aci.data(),
                              av.empty() ? &e_val : av.data(), 0};
             st = build_from_QAbc(&q, &a, c + v0, r1 > r0 ? AL + r0 : nullptr, r1 > r0 ? AU + r0 : nullptr, l + v0,
-                                 u + v0, obj_constants ? obj_constants[kb + k] : 0.0, &b->models[k]);
+                                 u + v0, obj_constants ? obj_constants[kk] : 0.0, &b->models[k]);
             st_k[k] = st;
             if (st == HPRQP_STATUS_OK) {
                 // record which original rows survived preprocessing
@@ -2432,14 +2443,51 @@ namespace hpr {
 
 // The one-call form of a large batch in two launches, so that the host's
 // preprocessing and upload of the second part run while the GPU solves the
-// first: the first part (about a quarter of the work, by nonzeros) is built
-// and launched, the rest is built and uploaded meanwhile and launched on its
-// own stream (its CTAs take the SMs as the first launch's CTAs finish), and
-// the results of both land in the caller's arrays.  Each instance is solved
-// by one CTA of the shape a single launch would use (batches this large take
-// 1024-thread CTAs), so the results equal a single launch's bit for bit;
-// each launch keeps its own time limit.
+// first.  The first part is the smallest instances, up to kFirstPartWork of
+// the nonzeros: they are quick to build, so their launch starts early, and
+// they are the ones whose iteration counts vary most (a small instance can
+// run a hundred times the median count, and such a straggler, started late,
+// would end the call late).  The rest is built and uploaded meanwhile and
+// launched on its own stream (its CTAs take the SMs as the first launch's
+// CTAs finish); each part's results are scattered back to the caller's
+// packing.  Each instance is solved by one CTA of the shape a single launch
+// would use (batches this large take 1024-thread CTAs), so the results equal
+// a single launch's bit for bit; each launch keeps its own time limit.
 constexpr size_t kSplitMinInstances = 1024;
+constexpr double kFirstPartWork = 0.15;
+
+// Results of a batch built from the caller's instances ids[0..K) (in that
+// order), written to the caller's packed arrays.
+static HPRQPStatus scatter_results(const HPRQPBatch *b, const std::vector<size_t> &ids, const size_t *var_offsets,
+                                   const size_t *row_offsets, int *status, size_t *iter, double *primal_obj,
+                                   double *residual, double *gap, double *x, double *y, double *z, double *w)
+{
+    const size_t K = ids.size(), nb = b->var_off[K], mb = b->row_off[K];
+    std::vector<int> st_b(status ? K : 0);
+    std::vector<size_t> it_b(iter ? K : 0);
+    std::vector<double> po_b(primal_obj ? K : 0), re_b(residual ? K : 0), ga_b(gap ? K : 0);
+    std::vector<double> x_b(x ? nb : 0), y_b(y ? mb : 0), z_b(z ? nb : 0), w_b(w ? nb : 0);
+    auto ptr = [](auto &v, const void *want) { return want ? v.data() : nullptr; };
+    HPRQPStatus st = hprqp_batch_get_results(b, ptr(st_b, status), ptr(it_b, iter), ptr(po_b, primal_obj),
+                                             ptr(re_b, residual), ptr(ga_b, gap), ptr(x_b, x), ptr(y_b, y),
+                                             ptr(z_b, z), ptr(w_b, w));
+    if (st != HPRQP_STATUS_OK) return st;
+    for (size_t j = 0; j < K; ++j) {
+        const size_t k = ids[j];
+        if (status) status[k] = st_b[j];
+        if (iter) iter[k] = it_b[j];
+        if (primal_obj) primal_obj[k] = po_b[j];
+        if (residual) residual[k] = re_b[j];
+        if (gap) gap[k] = ga_b[j];
+        const size_t vj = b->var_off[j], nj = b->var_off[j + 1] - vj, rj = b->row_off[j],
+                     mj = b->row_off[j + 1] - rj;
+        if (x) memcpy(x + var_offsets[k], x_b.data() + vj, nj * sizeof(double));
+        if (z) memcpy(z + var_offsets[k], z_b.data() + vj, nj * sizeof(double));
+        if (w) memcpy(w + var_offsets[k], w_b.data() + vj, nj * sizeof(double));
+        if (y) memcpy(y + row_offsets[k], y_b.data() + rj, mj * sizeof(double));
+    }
+    return HPRQP_STATUS_OK;
+}
 
 static HPRQPStatus solve_batch_in_two(size_t K, const size_t *var_offsets, const size_t *row_offsets,
                                       const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c,
@@ -2450,21 +2498,30 @@ static HPRQPStatus solve_batch_in_two(size_t K, const size_t *var_offsets, const
 {
     auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
     const double t0 = now();
-    // split where the nonzeros of the first part reach a quarter of the total
-    auto weight = [&](size_t k) {
-        const size_t v0 = var_offsets[k], v1 = var_offsets[k + 1], r0 = row_offsets[k], r1 = row_offsets[k + 1];
-        return (double)(Q->row_ptr[v1] - Q->row_ptr[v0]) + 2.0 * (double)(A->row_ptr[r1] - A->row_ptr[r0]) +
-               (double)(v1 - v0);
-    };
+    // the instances by nonzeros (the measure of the kernel's work queue),
+    // smallest first; the first part takes them up to kFirstPartWork of the
+    // total, each part keeps the caller's order
+    std::vector<double> wk(K);
     double total = 0.0;
-    for (size_t k = 0; k < K; ++k) total += weight(k);
+    for (size_t k = 0; k < K; ++k) {
+        const size_t v0 = var_offsets[k], v1 = var_offsets[k + 1], r0 = row_offsets[k], r1 = row_offsets[k + 1];
+        wk[k] = (double)(Q->row_ptr[v1] - Q->row_ptr[v0]) + 2.0 * (double)(A->row_ptr[r1] - A->row_ptr[r0]) +
+                (double)(v1 - v0);
+        total += wk[k];
+    }
+    std::vector<size_t> by_size(K);
+    std::iota(by_size.begin(), by_size.end(), size_t(0));
+    std::stable_sort(by_size.begin(), by_size.end(), [&](size_t a, size_t b) { return wk[a] < wk[b]; });
     size_t K1 = 0;
-    for (double acc = 0.0; K1 < K - 1 && acc < 0.25 * total; ++K1) acc += weight(K1);
+    for (double acc = 0.0; K1 < K - 1 && acc < kFirstPartWork * total; ++K1) acc += wk[by_size[K1]];
     K1 = std::max<size_t>(K1, 1);
+    std::vector<size_t> ids[2];
+    ids[0].assign(by_size.begin(), by_size.begin() + K1);
+    ids[1].assign(by_size.begin() + K1, by_size.end());
+    for (auto &v : ids) std::sort(v.begin(), v.end());
     HPRQPBatch *b[2] = {nullptr, nullptr};
     SolveLaunch L[2];
     HPRQPStatus st = HPRQP_STATUS_OK;
-    const size_t first[2] = {0, K1}, count[2] = {K1, K - K1};
     int launched = 0;
     double t_create[2] = {0.0, 0.0};
     for (int part = 0; part < 2 && st == HPRQP_STATUS_OK; ++part) {
@@ -2472,7 +2529,8 @@ static HPRQPStatus solve_batch_in_two(size_t K, const size_t *var_offsets, const
         // both parts take the CTA shape the whole batch would take, so each
         // instance sums in the same order as in a single launch
         st = batch_create_impl(K, var_offsets, row_offsets, Q, A, c, AL, AU, l, u, obj_constants,
-                               params->device_number, false, &b[part], false, first[part], count[part], kBigCta);
+                               params->device_number, false, &b[part], false, 0, ids[part].size(), kBigCta,
+                               ids[part].data());
         t_create[part] = now() - tc;
         if (st == HPRQP_STATUS_OK) st = batch_launch(b[part], params, L[part]);
         if (st == HPRQP_STATUS_OK) ++launched;
@@ -2483,13 +2541,9 @@ static HPRQPStatus solve_batch_in_two(size_t K, const size_t *var_offsets, const
         if (st == HPRQP_STATUS_OK) st = s2;
     }
     const double t2 = now();
-    for (int part = 0; part < 2 && st == HPRQP_STATUS_OK; ++part) {
-        const size_t kb = first[part], v0 = var_offsets[kb], r0 = row_offsets[kb];
-        st = hprqp_batch_get_results(b[part], status ? status + kb : nullptr, iter ? iter + kb : nullptr,
-                                     primal_obj ? primal_obj + kb : nullptr, residual ? residual + kb : nullptr,
-                                     gap ? gap + kb : nullptr, x ? x + v0 : nullptr, y ? y + r0 : nullptr,
-                                     z ? z + v0 : nullptr, w ? w + v0 : nullptr);
-    }
+    for (int part = 0; part < 2 && st == HPRQP_STATUS_OK; ++part)
+        st = scatter_results(b[part], ids[part], var_offsets, row_offsets, status, iter, primal_obj, residual, gap, x,
+                             y, z, w);
     const double t3 = now();
     for (int part = 0; part < 2; ++part) {
         if (part >= launched && L[part].e0) cudaEventDestroy(L[part].e0);
@@ -2498,9 +2552,9 @@ static HPRQPStatus solve_batch_in_two(size_t K, const size_t *var_offsets, const
     }
     if (trace)
         fprintf(stderr,
-                "[hprqp-b200 batch] in two launches (%zu + %zu instances): create %.3f + %.3f s, until both kernels "
-                "end %.3f s, results %.3f s, destroy %.3f s\n",
-                count[0], count[1], t_create[0], t_create[1], t2 - t1 + (t1 - t0 - t_create[0] - t_create[1]),
+                "[hprqp-b200 batch] in two launches (%zu smallest + %zu instances): create %.3f + %.3f s, until both "
+                "kernels end %.3f s, results %.3f s, destroy %.3f s\n",
+                ids[0].size(), ids[1].size(), t_create[0], t_create[1], t2 - t1 + (t1 - t0 - t_create[0] - t_create[1]),
                 t3 - t2, now() - t3);
     return st;
 }

@@ -153,11 +153,13 @@ double hprqp_batch_last_backward_ms(const HPRQPBatch *batch);
 void hprqp_batch_destroy(HPRQPBatch *batch);
 
 /* One-call form: create + solve + get_results + destroy.  A batch of 1024
- * instances or more is built and launched in two parts (about a quarter of
- * the work first), so that the host's preprocessing and upload of the rest
- * overlap the GPU's solve of the first part; the results are the same, bit
- * for bit, as those of a handle created with hprqp_batch_create and solved
- * with hprqp_batch_solve, and time_limit applies to each part's launch. */
+ * instances or more is built and launched in two parts -- first its smallest
+ * instances, up to 15 % of the nonzeros, then the rest -- so that the host's
+ * preprocessing and upload of the rest overlap the GPU's solve of the first
+ * part, and the small instances, whose iteration counts vary most, start
+ * early; the results are the same, bit for bit, as those of a handle created
+ * with hprqp_batch_create and solved with hprqp_batch_solve, and time_limit
+ * applies to each part's launch. */
 HPRQPStatus hprqp_solve_batch(size_t num_instances, const size_t *var_offsets, const size_t *row_offsets,
                               const HPRQPMatrixCSR *Q, const HPRQPMatrixCSR *A, const double *c, const double *AL,
                               const double *AU, const double *l, const double *u, const double *obj_constants,

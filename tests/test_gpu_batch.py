@@ -262,3 +262,44 @@ def test_one_call_equals_batch_handle(engine_lib, count):
     assert np.array_equal(one["obj"], r.objective)
     for key, ref in (("x", r.x), ("y", r.y), ("z", r.z), ("w", r.w)):
         assert np.array_equal(one[key], ref), key
+
+
+def test_one_call_split_mixed_sizes(engine_lib):
+    """The two-part one-call form on 1100 instances of mixed sizes (2 to 500
+    variables), a third of the small ones with a free row that preprocessing
+    removes: the first part takes the smallest instances, scattered through
+    the caller's order, and every result still lands in the caller's packing
+    bit for bit as a Batch handle gives it (removed rows: y = 0)."""
+    import dataclasses
+
+    from hprqp import batch
+
+    insts = []
+    for i in range(1100):
+        if i % 5 == 0:
+            insts.append(instances.config4_instance(i))
+        elif i % 5 == 1:
+            insts.append(TINY[i % len(TINY)])
+        else:
+            inst = instances.adjoint_case(i)
+            if i % 3 == 0:
+                AL, AU = inst.AL.copy(), inst.AU.copy()
+                AL[-1], AU[-1] = -np.inf, np.inf
+                inst = dataclasses.replace(inst, AL=AL, AU=AU)
+            insts.append(inst)
+    packed = batch.pack(insts)
+    one = _one_call(engine_lib, packed, stoptol=1e-6)
+    b = batch.Batch(packed)
+    b.solve(stoptol=1e-6)
+    r = b.results()
+    b.close()
+    assert np.array_equal(one["status"], r.status)
+    assert np.array_equal(one["iter"].astype(np.int64), r.iter)
+    assert np.array_equal(one["obj"], r.objective)
+    assert np.array_equal(one["res"], r.residual, equal_nan=True)
+    assert np.array_equal(one["gap"], r.gap, equal_nan=True)
+    for key, ref in (("x", r.x), ("y", r.y), ("z", r.z), ("w", r.w)):
+        assert np.array_equal(one[key], ref), key
+    row_end = np.asarray(packed.row_offsets)[1:]
+    freed = [k for k in range(1100) if k % 5 >= 2 and k % 3 == 0]  # adjoint cases, last row free
+    assert np.all(one["y"][row_end[freed] - 1] == 0.0)
