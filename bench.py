@@ -43,11 +43,11 @@ sys.path.insert(0, str(ROOT / "oracle"))
 
 # DRAM bytes moved per algorithmic byte by k_batch_solve: ncu on a 300-QP
 # launch of this workload in the bench's kernel shape (1024-thread CTAs, one
-# instance per SM at a time) read+wrote 359.018 + 26.762 GB
-# (dram__bytes_read.sum + dram__bytes_write.sum) for 512.257 GB of
+# instance per SM at a time, no shared-memory pool) read+wrote 348.288 +
+# 36.253 GB (dram__bytes_read.sum + dram__bytes_write.sum) for 512.257 GB of
 # algorithmic bytes; traffic grows with instance-iterations, so the bench
 # scales this ratio by its own launch's algorithmic bytes.
-BATCH_DRAM_PER_ALGO_BYTE = 385.780e9 / 512.257e9
+BATCH_DRAM_PER_ALGO_BYTE = 384.541e9 / 512.257e9
 METRIC = "solves/s to 1e-6 rel-KKT, batched vs plain on 1 B200; SpMV GB/s vs HBM peak"
 STOPTOL = 1e-6
 BATCH = 4096
