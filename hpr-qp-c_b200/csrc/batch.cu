@@ -55,8 +55,19 @@ namespace hpr {
 #ifndef HPR_BATCH_VEC_SMEM
 #define HPR_BATCH_VEC_SMEM 1
 #endif
-constexpr int kBigCta = 1024, kSmallCta = 512;
+constexpr int kBigCta = 1024, kMidCta = 640, kSmallCta = 512;
 constexpr int ctas_per_sm(int bt) { return bt >= 1024 ? 1 : 1024 / bt; }
+// In a batch of 1024-thread CTAs, an instance with n, m <= kMidCta (every
+// vector loop one entry per thread) and work (nnz(Q) + 2 nnz(A) + n of the
+// preprocessed model) at most kMidCtaMaxWork is solved by a 640-thread CTA
+// (96 registers against 64, one CTA per SM either way), in a launch of its
+// own started first (batch_launch).  Per-iteration times on the 4096-QP
+// batch recipe: 640 threads 18-24 % faster for n < 640, even or slower
+// above (each vector loop takes two passes), 7-15 % slower for work above
+// 40,000; 768 and 512 threads gave smaller and larger versions of the same
+// trade.  The rule is per instance, so an instance takes the same shape in
+// every batch of 1024-thread CTAs.
+constexpr long long kMidCtaMaxWork = 30000;
 // dynamic shared memory per CTA: the gathered vectors move to shared memory
 // when they fit and the pool leaves L1 large (batch_launch), else they stay
 // in global memory (L1-cached)
@@ -1462,7 +1473,11 @@ struct HPRQPBatch {
     int device = 0;
     int num_sms = 148;
     int cta_threads = 1024;  // threads per CTA of the solve and adjoint kernels (kBigCta or kSmallCta)
-    cudaStream_t stream = nullptr;
+    // kBigCta batches: the last k_mid instances of the work order are solved
+    // by kMidCta CTAs in a launch of their own on stream_mid
+    size_t k_mid = 0;
+    cudaStream_t stream = nullptr, stream_mid = nullptr;
+    int ws_slots = 0, phase_slots = 0;  // per-CTA workspaces and phase counters allocated
     size_t K = 0;
     std::vector<size_t> var_off, row_off;          // original packing (caller's layout)
     std::vector<int> n_k, m_k;                      // preprocessed sizes
@@ -1554,7 +1569,8 @@ static void batch_free(HPRQPBatch *b)
     for (auto &m : b->models) model_free(&m);
     b->models.clear();
     if (b->stream) cudaStreamDestroy(b->stream);
-    b->stream = nullptr;
+    if (b->stream_mid) cudaStreamDestroy(b->stream_mid);
+    b->stream = b->stream_mid = nullptr;
 }
 
 // The per-instance SpMV autotuner: the lane-group width of cta_spmv for one
@@ -1648,6 +1664,20 @@ void hprqp_batch_params_set_defaults(HPRQPBatchParams *p)
     p->print_frequency = -1;
     p->use_scaling = 1;
     p->device_number = 0;
+}
+
+// an instance's work measure: nonzeros the products of one HPR step stream,
+// plus its variables
+static long long instance_work(const HPRQPModel &M)
+{
+    return (long long)M.Q.nnz + 2 * (long long)M.A.nnz + (long long)M.Q.ncol;
+}
+
+// whether an instance of a batch of 1024-thread CTAs is solved by a kMidCta CTA
+static bool mid_cta_instance(const HPRQPModel &M)
+{
+    using namespace hpr;
+    return M.Q.ncol <= (size_t)kMidCta && M.A.nrow <= (size_t)kMidCta && instance_work(M) <= kMidCtaMaxWork;
 }
 
 static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const size_t *row_offsets,
@@ -1834,9 +1864,10 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     for (size_t k = tix; k < K; k += nth) {
         const HPRQPModel &M = b->models[k];
         BInst &I = b->inst[k];
-        I.q_lg = b->tuned_lg[3 * k] = choose_lane_group(M.Q.row_ptr, (int)M.Q.nrow, b->cta_threads / 32);
-        I.a_lg = b->tuned_lg[3 * k + 1] = choose_lane_group(M.A.row_ptr, (int)M.A.nrow, b->cta_threads / 32);
-        I.at_lg = b->tuned_lg[3 * k + 2] = choose_lane_group(M.AT.row_ptr, (int)M.AT.nrow, b->cta_threads / 32);
+        const int warps = (b->cta_threads == kBigCta && mid_cta_instance(M) ? kMidCta : b->cta_threads) / 32;
+        I.q_lg = b->tuned_lg[3 * k] = choose_lane_group(M.Q.row_ptr, (int)M.Q.nrow, warps);
+        I.a_lg = b->tuned_lg[3 * k + 1] = choose_lane_group(M.A.row_ptr, (int)M.A.nrow, warps);
+        I.at_lg = b->tuned_lg[3 * k + 2] = choose_lane_group(M.AT.row_ptr, (int)M.AT.nrow, warps);
         for (size_t r = 0; r <= M.Q.nrow; ++r) h_qrp[I.q_rp + r] = (int)M.Q.row_ptr[r];
         for (size_t r = 0; r <= M.A.nrow; ++r) h_arp[I.a_rp + r] = (int)M.A.row_ptr[r];
         for (size_t r = 0; r <= M.AT.nrow; ++r) h_atrp[I.at_rp + r] = (int)M.AT.row_ptr[r];
@@ -1884,7 +1915,8 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     };
     if (cudaSetDevice(device_number) != cudaSuccess ||
         cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device_number) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream_mid, cudaStreamNonBlocking) != cudaSuccess)
         return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
     BatchArgs &G = b->args;
     G.K = (int)K;
@@ -1898,20 +1930,27 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
     cv.add(&d_atci, h_atci.size()).add(&d_qv0, h_qv.size()).add(&d_av0, h_av.size()).add(&d_atv0, h_atv.size());
     cv.add(&G.q_v, h_qv.size()).add(&G.a_v, h_av.size()).add(&G.at_v, h_atv.size());
     cv.add(&d_c, h_c.size()).add(&d_l, h_l.size()).add(&d_u, h_u.size()).add(&d_AL, h_AL.size()).add(&d_AU, h_AU.size());
-    cv.add(&d_inst, K).add(&d_order, K).add(&d_counter, 1);
+    cv.add(&d_inst, K).add(&d_order, 2 * K).add(&d_counter, 2);
     cv.add(&G.x, h_c.size()).add(&G.z, h_c.size()).add(&G.w, h_c.size()).add(&G.y, h_AL.size());
     cv.add(&G.status, K).add(&G.iters, K).add(&G.pobj, K).add(&G.resid, K).add(&G.gap, K).add(&G.restarts, K);
     cv.add(&G.sigma_out, K).add(&G.seconds_out, K).add(&G.active_x, h_c.size()).add(&G.active_r, h_AL.size());
     cv.add(&G.col_norm_out, h_c.size()).add(&G.row_norm_out, h_AL.size()).add(&b->d_t0, 1);
     if ((st = cv.commit(b))) return fail(st);
-    // largest instances first
-    std::vector<int> order(K);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        const long long wx = b->models[x].Q.nnz + 2 * b->models[x].A.nnz + b->models[x].Q.ncol;
-        const long long wy = b->models[y].Q.nnz + 2 * b->models[y].A.nnz + b->models[y].Q.ncol;
-        return wx > wy;
-    });
+    // work orders, largest instances first: the adjoint's (second half of
+    // d_order) over all instances; the solve's (first half) the same with,
+    // in a kBigCta batch, the k_mid instances for kMidCta CTAs moved to its
+    // end -- the kBigCta launch takes the first K - k_mid entries, the
+    // kMidCta launch the rest, each as a queue with two ends
+    std::vector<int> order(2 * K);
+    std::iota(order.begin(), order.begin() + K, 0);
+    std::stable_sort(order.begin(), order.begin() + K,
+                     [&](int x, int y) { return instance_work(b->models[x]) > instance_work(b->models[y]); });
+    std::copy(order.begin(), order.begin() + K, order.begin() + K);
+    b->k_mid = 0;
+    if (b->cta_threads == kBigCta) {
+        std::stable_partition(order.begin(), order.begin() + K, [&](int k) { return !mid_cta_instance(b->models[k]); });
+        for (size_t k = 0; k < K; ++k) b->k_mid += mid_cta_instance(b->models[k]);
+    }
     auto up = [&](void *d, const void *h, size_t bytes) {
         return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, b->stream) == cudaSuccess;
     };
@@ -1922,7 +1961,7 @@ static HPRQPStatus batch_create_impl(size_t K, const size_t *var_offsets, const 
         !up(d_c, h_c.data(), h_c.size() * 8) || !up(d_l, h_l.data(), h_l.size() * 8) ||
         !up(d_u, h_u.data(), h_u.size() * 8) || !up(d_AL, h_AL.data(), h_AL.size() * 8) ||
         !up(d_AU, h_AU.data(), h_AU.size() * 8) || !up(d_inst, b->inst.data(), K * sizeof(BInst)) ||
-        !up(d_order, order.data(), K * sizeof(int)) || cudaStreamSynchronize(b->stream) != cudaSuccess)
+        !up(d_order, order.data(), 2 * K * sizeof(int)) || cudaStreamSynchronize(b->stream) != cudaSuccess)
         return fail(HPRQP_STATUS_NOT_IMPLEMENTED);
     // the abort flag (host-mapped memory) exists only for batches a caller
     // holds a handle to: the one-call forms cannot be asked to stop
@@ -1973,50 +2012,92 @@ HPRQPStatus hprqp_batch_create(size_t K, const size_t *var_offsets, const size_t
 
 namespace hpr {
 
-// a launched solve (batch_launch) waiting for batch_finish
+// a launched solve (batch_launch) waiting for batch_finish: one launch, or
+// two (segments of the work order) timed from one start event
 struct SolveLaunch {
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e0 = nullptr, e1[2] = {nullptr, nullptr};
     unsigned long long *d_phase = nullptr;
-    int grid = 0;
-    size_t smem = 0;
+    int segments = 0;
+    int bt[2] = {0, 0}, grid[2] = {0, 0};
+    size_t smem[2] = {0, 0};
 };
 
-// Start the solve kernel of a batch on its stream and return; the kernel's
-// events and optional phase clocks are in L.
+static void solve_launch_release(SolveLaunch &L)
+{
+    if (L.e0) cudaEventDestroy(L.e0);
+    for (auto &e : L.e1)
+        if (e) cudaEventDestroy(e);
+    L.e0 = L.e1[0] = L.e1[1] = nullptr;
+}
+
+// Start the solve of a batch and return; the launches' events and optional
+// phase clocks are in L.  A kBigCta batch with instances of work <=
+// kMidCtaMaxWork runs them first, in a kMidCta launch on the batch's stream,
+// and the others in a kBigCta launch on stream_mid: the mid-size CTAs (one
+// per SM) start every small instance at once -- the ones whose iteration
+// counts vary most -- and the 1024-thread CTAs take the SMs as they finish.
 static HPRQPStatus batch_launch(HPRQPBatch *b, const HPRQPBatchParams *p, SolveLaunch &L)
 {
     B_CK(cudaSetDevice(b->device));
     BatchArgs &G = b->args;
     const size_t na = ((size_t)G.nmax + 31) & ~size_t(31), ma = ((size_t)G.mmax + 31) & ~size_t(31);
     const size_t vec_bytes = (4 * na + 2 * ma) * sizeof(double);  // the gathered vectors
-    const int bt = b->cta_threads;
-    auto kern = bt == kBigCta ? k_batch_solve<kBigCta> : k_batch_solve<kSmallCta>;
-    // The gathered vectors go to shared memory only while the carveout that
-    // takes leaves most of the SM's 256 KB of unified L1 / shared memory to
-    // L1, which holds the instance's other vectors and its matrices: at most
-    // kPoolPerSm bytes of shared memory per SM (static and reserved bytes of
-    // every resident CTA included).  Measured on the 4096-QP batch (n up to
-    // 2000: 99.5 KB per SM with the pool) the pool made the mid-size
-    // instances whose whole working set fits a 248 KB L1 (n ~ 500) 5 % slower
-    // and the large ones 4 % faster; on 296 large QPs (two CTAs per SM, 195
-    // KB) it cost 12 %; on 256 QPs of n = 500 (48 KB) it saved 12 %.
-    cudaFuncAttributes fa;
-    B_CK(cudaFuncGetAttributes(&fa, kern));
-    const size_t pool_per_sm = (size_t)ctas_per_sm(bt) * (vec_bytes + fa.sharedSizeBytes + kReservedSmemPerCta);
-    G.vec_smem = HPR_BATCH_VEC_SMEM && vec_bytes <= smem_limit(bt) && pool_per_sm <= kPoolPerSm;
-    const size_t smem = G.vec_smem ? vec_bytes : 0;
-    B_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, bt, smem));
-    const int grid = std::max(1, std::min((int)b->K, b->num_sms * std::max(per_sm, 1)));
-    // per-CTA workspace (allocated lazily, sized by the grid)
+    struct Seg {
+        size_t first, count;  // entries of the work order
+        int bt;
+        cudaStream_t stream;
+    };
+    Seg seg[2];
+    int ns = 0;
+    const size_t k_big = b->K - b->k_mid;
+    if (b->k_mid > 0) {
+        seg[ns] = {k_big, b->k_mid, kMidCta, b->stream};
+        ++ns;
+    }
+    if (k_big > 0) {
+        seg[ns] = {0, k_big, b->cta_threads, ns == 0 ? b->stream : b->stream_mid};
+        ++ns;
+    }
+    L.segments = ns;
+    auto kern_of = [](int bt) {
+        return bt == kBigCta ? k_batch_solve<kBigCta> : bt == kMidCta ? k_batch_solve<kMidCta> : k_batch_solve<kSmallCta>;
+    };
+    int vec_smem[2] = {0, 0}, slots = 0, off[2] = {0, 0};
+    for (int s = 0; s < ns; ++s) {
+        const int bt = seg[s].bt;
+        auto kern = kern_of(bt);
+        // The gathered vectors go to shared memory only while the carveout
+        // that takes leaves most of the SM's 256 KB of unified L1 / shared
+        // memory to L1, which holds the instance's other vectors and its
+        // matrices: at most kPoolPerSm bytes of shared memory per SM (static
+        // and reserved bytes of every resident CTA included).  Measured on
+        // the 4096-QP batch (n up to 2000: 99.5 KB per SM with the pool) the
+        // pool made the mid-size instances whose whole working set fits a
+        // 248 KB L1 (n ~ 500) 5 % slower and the large ones 4 % faster; on
+        // 296 large QPs (two CTAs per SM, 195 KB) it cost 12 %; on 256 QPs of
+        // n = 500 (48 KB) it saved 12 %.
+        cudaFuncAttributes fa;
+        B_CK(cudaFuncGetAttributes(&fa, kern));
+        const size_t pool_per_sm = (size_t)ctas_per_sm(bt) * (vec_bytes + fa.sharedSizeBytes + kReservedSmemPerCta);
+        vec_smem[s] = HPR_BATCH_VEC_SMEM && vec_bytes <= smem_limit(bt) && pool_per_sm <= kPoolPerSm;
+        L.smem[s] = vec_smem[s] ? vec_bytes : 0;
+        B_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem[s]));
+        int per_sm = 0;
+        B_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, bt, L.smem[s]));
+        L.bt[s] = bt;
+        L.grid[s] = std::max(1, std::min((int)seg[s].count, b->num_sms * std::max(per_sm, 1)));
+        off[s] = slots;
+        slots += L.grid[s];
+    }
+    // per-CTA workspace of every launch (allocated lazily, kept for the next solves)
     const size_t stride = kBatchNVecs * na + kBatchMVecs * ma;
-    if (!G.ws || G.ws_stride != stride) {
+    if (!G.ws || G.ws_stride != stride || b->ws_slots < slots) {
         double *ws = nullptr;
-        HPRQPStatus st = balloc(b, &ws, stride * (size_t)b->num_sms * std::max(per_sm, 1));
+        HPRQPStatus st = balloc(b, &ws, stride * (size_t)slots);
         if (st) return st;
         G.ws = ws;
         G.ws_stride = stride;
+        b->ws_slots = slots;
     }
     G.stoptol = p->stoptol;
     G.max_iter = (long long)std::min<size_t>(p->max_iter, (size_t)LLONG_MAX);
@@ -2025,67 +2106,88 @@ static HPRQPStatus batch_launch(HPRQPBatch *b, const HPRQPBatchParams *p, SolveL
     G.print_frequency = p->print_frequency;
     G.use_scaling = p->use_scaling;
     unsigned long long *d_t0 = b->d_t0;
-    B_CK(cudaMemsetAsync(G.counter, 0, sizeof(*G.counter), b->stream));
+    B_CK(cudaMemsetAsync(G.counter, 0, 2 * sizeof(*G.counter), b->stream));
     k_batch_clock<<<1, 1, 0, b->stream>>>(d_t0);
     count_launch();
     unsigned long long h_t0 = 0;
     B_CK(cudaMemcpyAsync(&h_t0, d_t0, sizeof(h_t0), cudaMemcpyDeviceToHost, b->stream));
     B_CK(cudaStreamSynchronize(b->stream));
     G.t_start = h_t0;
-    cudaEvent_t &e0 = L.e0, &e1 = L.e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, b->stream);
     const char *pe = getenv("HPRQP_B200_BATCH_PHASES");
     unsigned long long *d_phase = nullptr;
     if (pe && pe[0] == '1') {
-        if (!b->d_phase) {
-            HPRQPStatus st2 = balloc(b, &b->d_phase, (size_t)grid * 8);
+        if (!b->d_phase || b->phase_slots < slots) {
+            HPRQPStatus st2 = balloc(b, &b->d_phase, (size_t)slots * 8);
             if (st2) return st2;
+            b->phase_slots = slots;
         }
         d_phase = b->d_phase;
-        B_CK(cudaMemsetAsync(d_phase, 0, (size_t)grid * 8 * sizeof(unsigned long long), b->stream));
+        B_CK(cudaMemsetAsync(d_phase, 0, (size_t)slots * 8 * sizeof(unsigned long long), b->stream));
     }
-    G.phase_clk = d_phase;
-    kern<<<grid, bt, smem, b->stream>>>(G);
-    count_launch();
-    cudaEventRecord(e1, b->stream);
     L.d_phase = d_phase;
-    L.grid = grid;
-    L.smem = smem;
+    B_CK(cudaEventCreate(&L.e0));
+    for (int s = 0; s < ns; ++s) B_CK(cudaEventCreate(&L.e1[s]));
+    B_CK(cudaEventRecord(L.e0, b->stream));
+    cudaError_t err = cudaSuccess;
+    for (int s = 0; s < ns && err == cudaSuccess; ++s) {
+        BatchArgs A = G;
+        A.K = (int)seg[s].count;
+        A.order = G.order + seg[s].first;
+        A.counter = G.counter + s;
+        A.ws = G.ws + (size_t)off[s] * stride;
+        A.vec_smem = vec_smem[s];
+        A.phase_clk = d_phase ? d_phase + (size_t)off[s] * 8 : nullptr;
+        if (seg[s].stream != b->stream) err = cudaStreamWaitEvent(seg[s].stream, L.e0, 0);
+        if (err != cudaSuccess) break;
+        kern_of(seg[s].bt)<<<L.grid[s], seg[s].bt, L.smem[s], seg[s].stream>>>(A);
+        count_launch();
+        err = cudaGetLastError();
+        if (err == cudaSuccess) err = cudaEventRecord(L.e1[s], seg[s].stream);
+    }
+    if (err != cudaSuccess) {
+        // nothing launched may still run when the caller frees the batch
+        cudaStreamSynchronize(b->stream);
+        cudaStreamSynchronize(b->stream_mid);
+        B_CK(err);
+    }
     return HPRQP_STATUS_OK;
 }
 
-// Wait for a launched solve, record its device time, print the optional
-// phase clocks.
+// Wait for a launched solve, record its device time (start event to the end
+// of the last launch), print the optional phase clocks.
 static HPRQPStatus batch_finish(HPRQPBatch *b, SolveLaunch &L)
 {
-    cudaEvent_t e0 = L.e0, e1 = L.e1;
-    unsigned long long *d_phase = L.d_phase;
-    const int grid = L.grid;
-    const size_t smem = L.smem;
     B_CK(cudaSetDevice(b->device));
-    cudaError_t err = cudaEventSynchronize(e1);
+    cudaError_t err = cudaSuccess;
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    for (int s = 0; s < L.segments; ++s) {
+        const cudaError_t e = cudaEventSynchronize(L.e1[s]);
+        if (err == cudaSuccess) err = e;
+        float t = 0.f;
+        if (e == cudaSuccess && cudaEventElapsedTime(&t, L.e0, L.e1[s]) == cudaSuccess) ms = std::max(ms, t);
+    }
+    solve_launch_release(L);
     B_CK(err);
     B_CK(cudaGetLastError());
     b->last_ms = ms;
     b->solved = true;
     // an abort request ends with the solve it stopped
     if (b->h_abort) __atomic_store_n(b->h_abort, 0, __ATOMIC_SEQ_CST);
-    if (d_phase) {
-        std::vector<unsigned long long> h((size_t)grid * 8);
-        B_CK(cudaMemcpy(h.data(), d_phase, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    if (L.d_phase) {
+        int slots = 0;
+        for (int s = 0; s < L.segments; ++s) slots += L.grid[s];
+        std::vector<unsigned long long> h((size_t)slots * 8);
+        B_CK(cudaMemcpy(h.data(), L.d_phase, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         double tot[8] = {0};
-        for (int g = 0; g < grid; ++g)
+        for (int g = 0; g < slots; ++g)
             for (int q = 0; q < 8; ++q) tot[q] += (double)h[(size_t)g * 8 + q];
         fprintf(stderr, "[hprqp-b200 batch phases, %% of CTA time] load+scale %.1f setup %.1f power %.1f steps %.1f "
-                        "residuals %.1f m-norm %.1f sigma+restart %.1f (grid %d, smem %zu)\n",
+                        "residuals %.1f m-norm %.1f sigma+restart %.1f (",
                 100 * tot[0] / tot[7], 100 * tot[1] / tot[7], 100 * tot[2] / tot[7], 100 * tot[3] / tot[7],
-                100 * tot[4] / tot[7], 100 * tot[5] / tot[7], 100 * tot[6] / tot[7], grid, smem);
+                100 * tot[4] / tot[7], 100 * tot[5] / tot[7], 100 * tot[6] / tot[7]);
+        for (int s = 0; s < L.segments; ++s)
+            fprintf(stderr, "%s%d CTAs of %d threads, smem %zu", s ? "; " : "", L.grid[s], L.bt[s], L.smem[s]);
+        fprintf(stderr, ")\n");
     }
     return HPRQP_STATUS_OK;
 }
@@ -2101,8 +2203,7 @@ HPRQPStatus hprqp_batch_solve(HPRQPBatch *b, const HPRQPBatchParams *p)
     SolveLaunch L;
     HPRQPStatus st = batch_launch(b, p, L);
     if (st != HPRQP_STATUS_OK) {
-        if (L.e0) cudaEventDestroy(L.e0);
-        if (L.e1) cudaEventDestroy(L.e1);
+        solve_launch_release(L);
         return st;
     }
     return batch_finish(b, L);
@@ -2312,7 +2413,7 @@ HPRQPStatus hprqp_batch_backward(HPRQPBatch *b, const double *grad_x, const doub
     AdjArgs A{};
     A.K = (int)K;
     A.inst = G.inst;
-    A.order = G.order;
+    A.order = G.order + K;  // the adjoint's work order: all instances, largest first
     A.counter = b->adj_counter;
     A.q_rp = G.q_rp;
     A.q_ci = G.q_ci;
@@ -2546,8 +2647,7 @@ static HPRQPStatus solve_batch_in_two(size_t K, const size_t *var_offsets, const
                              y, z, w);
     const double t3 = now();
     for (int part = 0; part < 2; ++part) {
-        if (part >= launched && L[part].e0) cudaEventDestroy(L[part].e0);
-        if (part >= launched && L[part].e1) cudaEventDestroy(L[part].e1);
+        if (part >= launched) solve_launch_release(L[part]);
         if (b[part]) hprqp_batch_destroy(b[part]);
     }
     if (trace)

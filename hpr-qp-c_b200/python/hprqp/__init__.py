@@ -215,13 +215,16 @@ def _spmv_mode_code(value) -> int:
 class Model:
     def __init__(self) -> None:
         handle = ctypes.c_void_p()
-        _raise_for_status(_lib().hprqp_model_create(ctypes.byref(handle)), "hprqp_model_create")
+        self._lib_ref = _lib()
+        _raise_for_status(self._lib_ref.hprqp_model_create(ctypes.byref(handle)), "hprqp_model_create")
         self._handle = handle
 
     def __del__(self) -> None:
-        handle = getattr(self, "_handle", None)
-        if handle is not None and handle.value and _Library._instance is not None:
-            _Library._instance.hprqp_model_destroy(handle)
+        # the library handle is read from the instance: at interpreter exit
+        # the module's globals may already be gone
+        handle, lib = getattr(self, "_handle", None), getattr(self, "_lib_ref", None)
+        if handle is not None and handle.value and lib is not None:
+            lib.hprqp_model_destroy(handle)
             handle.value = None
 
     @property
@@ -263,15 +266,18 @@ class Model:
 class Parameters:
     def __init__(self, **kwargs) -> None:
         handle = ctypes.c_void_p()
-        _raise_for_status(_lib().hprqp_params_create(ctypes.byref(handle)), "hprqp_params_create")
+        self._lib_ref = _lib()
+        _raise_for_status(self._lib_ref.hprqp_params_create(ctypes.byref(handle)), "hprqp_params_create")
         self._handle = handle
         for name, value in kwargs.items():
             getattr(self, f"set_{name}")(value)
 
     def __del__(self) -> None:
-        handle = getattr(self, "_handle", None)
-        if handle is not None and handle.value and _Library._instance is not None:
-            _Library._instance.hprqp_params_destroy(handle)
+        # the library handle is read from the instance: at interpreter exit
+        # the module's globals may already be gone
+        handle, lib = getattr(self, "_handle", None), getattr(self, "_lib_ref", None)
+        if handle is not None and handle.value and lib is not None:
+            lib.hprqp_params_destroy(handle)
             handle.value = None
 
     def _call(self, func_name: str, *args) -> "Parameters":
