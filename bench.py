@@ -42,12 +42,13 @@ sys.path.insert(0, str(ROOT / "hpr-qp-c_b200" / "python"))
 sys.path.insert(0, str(ROOT / "oracle"))
 
 # DRAM bytes moved per algorithmic byte by k_batch_solve: ncu on a 300-QP
-# launch of this workload in the bench's kernel shape (1024-thread CTAs, one
-# instance per SM at a time, no shared-memory pool) read+wrote 348.288 +
-# 36.253 GB (dram__bytes_read.sum + dram__bytes_write.sum) for 512.257 GB of
-# algorithmic bytes; traffic grows with instance-iterations, so the bench
-# scales this ratio by its own launch's algorithmic bytes.
-BATCH_DRAM_PER_ALGO_BYTE = 384.541e9 / 512.257e9
+# solve of this workload in the bench's kernel shapes (a 640-thread launch
+# for its 85 instances of n, m <= 640, a 1024-thread launch for the rest, one
+# instance per SM at a time, no shared-memory pool) read+wrote 0.009 +
+# 394.424 GB (dram__bytes_read.sum + dram__bytes_write.sum of both launches)
+# for 512.257 GB of algorithmic bytes; traffic grows with instance-iterations,
+# so the bench scales this ratio by its own solve's algorithmic bytes.
+BATCH_DRAM_PER_ALGO_BYTE = 394.433e9 / 512.257e9
 METRIC = "solves/s to 1e-6 rel-KKT, batched vs plain on 1 B200; SpMV GB/s vs HBM peak"
 STOPTOL = 1e-6
 BATCH = 4096
@@ -714,9 +715,11 @@ def main():
                     "optimal": e2e_ok},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": algo_bytes * BATCH_DRAM_PER_ALGO_BYTE,
-                         "traffic_source": "ncu DRAM bytes of a 300-QP launch of this workload (same kernel "
-                                           "shape), scaled by algorithmic bytes (instance-iterations)",
-                         "kernel": "k_batch_solve",
+                         "traffic_source": "ncu DRAM bytes of a 300-QP solve of this workload (same kernel "
+                                           "shapes), scaled by algorithmic bytes (instance-iterations)",
+                         "kernel": "k_batch_solve (one solve: a 640-thread launch for the instances of "
+                                   "n, m <= 640 and a 1024-thread launch for the rest, concurrent; "
+                                   "achieved over their span)",
                          "algorithmic_bytes_per_launch": algo_bytes, "peak_kind": peak_kind},
             "solved_optimal": int(np.sum(res.status == 6)), "mean_iters": float(iters.mean())}
 
