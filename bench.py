@@ -245,6 +245,21 @@ def objective_agreement(ours_status, ours_obj, ref_solved):
             "max_rel_objective_diff": float(max(diffs)) if diffs else None}
 
 
+def plain_call_stats(seconds, product_nnz, one_cta_limit: int = 200000):
+    """Per-call summary of the plain loop: median and slowest call, and the
+    slowest call's instance and route (solve_gpu runs a model without cones
+    on one CTA of the batch kernel when 2 nnz(Q) + 2 nnz(A) <= the limit,
+    else through the host-driven loop)."""
+    ms = [1e3 * float(t) for t in seconds]
+    if not ms:
+        return {"calls": 0}
+    k = int(np.argmax(ms))
+    route = lambda w: "one CTA" if w <= one_cta_limit else "host loop"  # noqa: E731
+    return {"calls": len(ms), "median_ms": round(float(np.median(ms)), 2), "max_ms": round(ms[k], 2),
+            "max_instance": k, "max_route": route(int(product_nnz[k])),
+            "host_loop_calls": int(sum(int(w) > one_cta_limit for w in product_nnz))}
+
+
 def cpu_model() -> str:
     try:
         for line in Path("/proc/cpuinfo").read_text().splitlines():
@@ -729,10 +744,14 @@ def main():
         models = [hprqp.build_from_instance(i) for i in sample]
         params = hprqp.Parameters(verbose=False, stoptol=STOPTOL, device_number=local_rank)
         hprqp.optimize(models[0], params)
+        call_s = []
         t0 = time.perf_counter()
         for mdl in models:
+            t1 = time.perf_counter()
             hprqp.optimize(mdl, params)
+            call_s.append(time.perf_counter() - t1)
         plain_rate = len(models) / (time.perf_counter() - t0)
+        calls = plain_call_stats(call_s, [2 * (i.Q.nnz + i.A.nnz) for i in sample])
         # the same loop through the host-driven route of solve_gpu (every
         # iteration launched from the host), which small QPs no longer take
         old_route = hprqp.set_single_cta_max_work(0)
@@ -746,7 +765,7 @@ def main():
             hprqp.set_single_cta_max_work(old_route)
         line["plain"] = {"value": plain_rate, "unit": "solves/s", "sample": f"{len(models)} instances of the batch",
                          "route": "one CTA of the batch kernel per solve_gpu call (small models)",
-                         "host_loop": host_loop_rate}
+                         "host_loop": host_loop_rate, "calls": calls}
         line["batched_over_plain"] = value / world / plain_rate
         line["batched_over_plain_host_loop"] = value / world / host_loop_rate
         if not args.no_spmv:

@@ -45,3 +45,15 @@ def test_objective_agreement_counts_only_both_optimal():
     assert got["instances"] == 3 and got["both_optimal"] == 2
     assert abs(got["max_rel_objective_diff"] - 1e-7) < 1e-12
     assert bench.objective_agreement(np.array([4]), np.array([0.0]), [(0, 6, 1.0)])["max_rel_objective_diff"] is None
+
+
+def test_plain_call_stats_names_the_slowest_call_and_its_route():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    got = bench.plain_call_stats([0.05, 0.06, 0.7, 0.055], [1000, 150000, 300000, 5000])
+    assert got["calls"] == 4 and got["max_instance"] == 2 and got["max_route"] == "host loop"
+    assert got["max_ms"] == 700.0 and got["median_ms"] == 57.5 and got["host_loop_calls"] == 1
+    assert bench.plain_call_stats([0.01], [200000])["max_route"] == "one CTA"
+    assert bench.plain_call_stats([], []) == {"calls": 0}
+
