@@ -46,9 +46,16 @@ HPRQPStatus hprqp_batch_create(size_t num_instances, const size_t *var_offsets, 
                                const double *AL, const double *AU, const double *l, const double *u,
                                const double *obj_constants, int device_number, HPRQPBatch **out);
 
-/* Solve all instances (one persistent kernel; inputs already on the device).
- * May be called repeatedly; every call starts from the original data, at
- * zero or at the point set by hprqp_batch_set_warm_start. */
+/* Solve all instances (inputs already on the device): persistent kernels,
+ * one instance per CTA, taken from a work queue with two ends (half the CTAs
+ * take the largest instance left, half the smallest).  In a batch of more
+ * than two instances per SM, the instances of at most 640 variables and 640
+ * rows with few nonzeros run in a launch of 640-thread CTAs started first,
+ * the others in a launch of 1024-thread CTAs beside it; the shape is fixed
+ * per instance, so an instance's result does not depend on the rest of the
+ * batch or on timing.  Returns when the solve has ended.  May be called
+ * repeatedly; every call starts from the original data, at zero or at the
+ * point set by hprqp_batch_set_warm_start. */
 HPRQPStatus hprqp_batch_solve(HPRQPBatch *batch, const HPRQPBatchParams *params);
 
 /* Start the following hprqp_batch_solve calls from a given point instead of
