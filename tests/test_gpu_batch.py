@@ -265,18 +265,22 @@ def test_one_call_equals_batch_handle(engine_lib, count):
 
 
 def test_one_call_split_mixed_sizes(engine_lib):
-    """The two-part one-call form on 1100 instances of mixed sizes (2 to 500
+    """The two-part one-call form on 1100 instances of mixed sizes (2 to 2000
     variables), a third of the small ones with a free row that preprocessing
     removes: the first part takes the smallest instances, scattered through
-    the caller's order, and every result still lands in the caller's packing
-    bit for bit as a Batch handle gives it (removed rows: y = 0)."""
+    the caller's order; instances of n, m <= 640 run on 640-thread CTAs and
+    the batch-recipe QPs (n up to 2000) mostly on 1024-thread CTAs, in both
+    parts and in the handle; every result still lands in the caller's
+    packing bit for bit as a Batch handle gives it (removed rows: y = 0)."""
     import dataclasses
 
     from hprqp import batch
 
     insts = []
     for i in range(1100):
-        if i % 5 == 0:
+        if i % 22 == 10:
+            insts.append(instances.config3_instance(i))
+        elif i % 5 == 0:
             insts.append(instances.config4_instance(i))
         elif i % 5 == 1:
             insts.append(TINY[i % len(TINY)])
@@ -301,5 +305,5 @@ def test_one_call_split_mixed_sizes(engine_lib):
     for key, ref in (("x", r.x), ("y", r.y), ("z", r.z), ("w", r.w)):
         assert np.array_equal(one[key], ref), key
     row_end = np.asarray(packed.row_offsets)[1:]
-    freed = [k for k in range(1100) if k % 5 >= 2 and k % 3 == 0]  # adjoint cases, last row free
+    freed = [k for k in range(1100) if k % 22 != 10 and k % 5 >= 2 and k % 3 == 0]  # adjoint cases, last row free
     assert np.all(one["y"][row_end[freed] - 1] == 0.0)
