@@ -1,5 +1,5 @@
-// Batched HPR-QP solver: one persistent kernel solves thousands of
-// independent QPs.
+// Batched HPR-QP solver: persistent kernels solve thousands of independent
+// QPs.
 //
 // Each CTA takes instances from a global work queue with two ends (even
 // CTAs take the largest instance left, odd CTAs the smallest, take_instance)
@@ -654,8 +654,9 @@ __global__ void __launch_bounds__(BT, ctas_per_sm(BT)) k_batch_solve(const Batch
             if (tid == 0) S.lQ = lq * 1.05;
         }
         {
-            // the products' sources in the slots of y_bar and w (shared
-            // memory), which the starting iterates below overwrite
+            // the products' sources in the slots of y_bar and w (in the
+            // shared-memory pool when there is one), which the starting
+            // iterates below overwrite
             const double la = m > 0 ? cta_power<kBT>(A, AT, Q, true, m, V.pz, V.y_bar, V.w, s_red, s_out) : 0.0;
             if (tid == 0) S.lA = la * 1.05;
         }
@@ -1473,8 +1474,9 @@ struct HPRQPBatch {
     int device = 0;
     int num_sms = 148;
     int cta_threads = 1024;  // threads per CTA of the solve and adjoint kernels (kBigCta or kSmallCta)
-    // kBigCta batches: the last k_mid instances of the work order are solved
-    // by kMidCta CTAs in a launch of their own on stream_mid
+    // kBigCta batches: the last k_mid instances of the solve's work order
+    // (mid_cta_instance) are solved by kMidCta CTAs in a launch of their own
+    // on `stream`, the others by kBigCta CTAs on stream_mid
     size_t k_mid = 0;
     cudaStream_t stream = nullptr, stream_mid = nullptr;
     int ws_slots = 0, phase_slots = 0;  // per-CTA workspaces and phase counters allocated
@@ -2031,9 +2033,9 @@ static void solve_launch_release(SolveLaunch &L)
 }
 
 // Start the solve of a batch and return; the launches' events and optional
-// phase clocks are in L.  A kBigCta batch with instances of work <=
-// kMidCtaMaxWork runs them first, in a kMidCta launch on the batch's stream,
-// and the others in a kBigCta launch on stream_mid: the mid-size CTAs (one
+// phase clocks are in L.  A kBigCta batch with instances for kMidCta CTAs
+// (mid_cta_instance) runs them first, in a kMidCta launch on the batch's
+// stream, and the others in a kBigCta launch on stream_mid: the mid-size CTAs (one
 // per SM) start every small instance at once -- the ones whose iteration
 // counts vary most -- and the 1024-thread CTAs take the SMs as they finish.
 static HPRQPStatus batch_launch(HPRQPBatch *b, const HPRQPBatchParams *p, SolveLaunch &L)
@@ -2542,7 +2544,7 @@ void hprqp_batch_destroy(HPRQPBatch *b)
 
 namespace hpr {
 
-// The one-call form of a large batch in two launches, so that the host's
+// The one-call form of a large batch in two parts, so that the host's
 // preprocessing and upload of the second part run while the GPU solves the
 // first.  The first part is the smallest instances, up to kFirstPartWork of
 // the nonzeros: they are quick to build, so their launch starts early, and
@@ -2552,8 +2554,10 @@ namespace hpr {
 // launched on its own stream (its CTAs take the SMs as the first launch's
 // CTAs finish); each part's results are scattered back to the caller's
 // packing.  Each instance is solved by one CTA of the shape a single launch
-// would use (batches this large take 1024-thread CTAs), so the results equal
-// a single launch's bit for bit; each launch keeps its own time limit.
+// would give it (batches this large take 1024-thread CTAs, and 640-thread
+// CTAs for the instances mid_cta_instance picks, a rule on the instance
+// alone), so the results equal a single launch's bit for bit; each launch
+// keeps its own time limit.
 constexpr size_t kSplitMinInstances = 1024;
 constexpr double kFirstPartWork = 0.15;
 
